@@ -1,0 +1,329 @@
+// Driver around the reference's own CPU implementation of the SIMPLE / p'
+// path, linked against oracle/_ref/libcfdref.a (built from the reference's
+// sources by oracle/Makefile.ref).  Test infrastructure only: it produces
+// golden vectors and the timed CPU baseline; the product never links it.
+//
+// Commands (key=value arguments, binary float64 outputs under out=DIR):
+//
+//   poisson dim=2|3 n=N [seed=S] [rtol=1e-8] [maxit=M] [pre=jacobi|none]
+//           [solver=cg|bicgstab] [out=DIR] [dump_matrix=1]
+//       p' system of the reference's assemblePressureCorrection
+//       (PressureCorrectionEquation.cpp:341) with unit response
+//       coefficients, rho = 1, all-FixedGradient(0) pressure patches and
+//       cell 0 pinned, on createCartesian2D(n,n,1,1) /
+//       createCartesian3D(n,n,n,1,1,1); RHS = oracle_synth_rhs(seed);
+//       solved by the reference CG (CG.cpp:14) + JacobiPreconditioner
+//       (Preconditioner.cpp:34) from x0 = 0 with absoluteTolerance = 0.
+//
+//   simple dim=2|3 nx= ny= [nz=] [lx=1 ly=1 lz=1] [rho=1] [mu=0.01]
+//          [flow=cavity|channel] [lid=1] [inlet=1] [au=0.7] [ap=0.3]
+//          [tolu=1e-6] [tolp=1e-6] [tolc=1e-6] [outer=N]
+//          [scheme=upwind|central|lud|quick] [flux=auto|linear|rhiechow]
+//          [mabs=1e-10] [mrel=1e-8] [mmax=500]
+//          [psolver=cg|bicgstab] [ppre=jacobi|none] [pabs=0] [prel=1e-8] [pmax=5000]
+//          [out=DIR]
+//       the reference SIMPLE::solve (SIMPLE.cpp:148) on a uniform Cartesian
+//       lid-driven cavity (Wall x3 + MovingWall{lid,0}) or channel (Inlet
+//       {inlet,0} left, Outlet right, Walls; pressure FixedValue(0) at the
+//       outlet), pressure FixedGradient(0) elsewhere.  Writes u v [w] p flux
+//       and the residual histories.
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <fstream>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "cfd/algebra/BiCGSTAB.hpp"
+#include "cfd/algebra/CG.hpp"
+#include "cfd/algebra/LinearSystem.hpp"
+#include "cfd/algebra/Preconditioner.hpp"
+#include "cfd/boundary/FixedGradient.hpp"
+#include "cfd/boundary/FixedValue.hpp"
+#include "cfd/boundary/Inlet.hpp"
+#include "cfd/boundary/MovingWall.hpp"
+#include "cfd/boundary/Outlet.hpp"
+#include "cfd/boundary/Wall.hpp"
+#include "cfd/fields/ScalarField.hpp"
+#include "cfd/fields/SurfaceField.hpp"
+#include "cfd/fields/VectorField.hpp"
+#include "cfd/mesh/MeshGeometry.hpp"
+#include "cfd/physics/FluidProperties.hpp"
+#include "cfd/pressure_velocity/PressureCorrectionEquation.hpp"
+#include "cfd/pressure_velocity/SIMPLE.hpp"
+#include "synth_rhs.h"
+
+using namespace cfd;
+
+namespace {
+
+using Args = std::map<std::string, std::string>;
+
+std::string get(const Args& a, const std::string& k, const std::string& d) {
+  auto it = a.find(k);
+  return it == a.end() ? d : it->second;
+}
+double getd(const Args& a, const std::string& k, double d) {
+  auto it = a.find(k);
+  return it == a.end() ? d : std::strtod(it->second.c_str(), nullptr);
+}
+long long geti(const Args& a, const std::string& k, long long d) {
+  auto it = a.find(k);
+  return it == a.end() ? d : std::strtoll(it->second.c_str(), nullptr, 10);
+}
+
+void writeBin(const std::string& path, const double* data, size_t n) {
+  std::ofstream f(path, std::ios::binary);
+  f.write(reinterpret_cast<const char*>(data), static_cast<std::streamsize>(n * sizeof(double)));
+}
+void writeBin(const std::string& path, const std::vector<double>& v) {
+  writeBin(path, v.data(), v.size());
+}
+
+const char* solverStatusText(algebra::SolverStatus s) {
+  switch (s) {
+    case algebra::SolverStatus::Converged: return "Converged";
+    case algebra::SolverStatus::MaxIterations: return "MaxIterations";
+    case algebra::SolverStatus::Breakdown: return "Breakdown";
+    case algebra::SolverStatus::NonFiniteInput: return "NonFiniteInput";
+    case algebra::SolverStatus::NonFiniteResidual: return "NonFiniteResidual";
+    case algebra::SolverStatus::InvalidSystem: return "InvalidSystem";
+  }
+  return "?";
+}
+
+const char* simpleStatusName(pressure_velocity::SIMPLEStatus s) {
+  using S = pressure_velocity::SIMPLEStatus;
+  switch (s) {
+    case S::Converged: return "Converged";
+    case S::MaxIterations: return "MaxIterations";
+    case S::MomentumFailure: return "MomentumFailure";
+    case S::PressureCorrectionFailure: return "PressureCorrectionFailure";
+    case S::NonFiniteState: return "NonFiniteState";
+    case S::InvalidConfiguration: return "InvalidConfiguration";
+    case S::Cancelled: return "Cancelled";
+    case S::Stagnated: return "Stagnated";
+    case S::Diverging: return "Diverging";
+  }
+  return "?";
+}
+
+mesh::Mesh makeMesh(int dim, long long nx, long long ny, long long nz, double lx, double ly,
+                    double lz) {
+  if (dim == 3) return mesh::MeshGeometry::createCartesian3D(nx, ny, nz, lx, ly, lz);
+  return mesh::MeshGeometry::createCartesian2D(nx, ny, lx, ly);
+}
+
+int runPoisson(const Args& a) {
+  const int dim = static_cast<int>(geti(a, "dim", 2));
+  const long long n = geti(a, "n", 64);
+  const auto seed = static_cast<uint64_t>(geti(a, "seed", 20261203));
+  const std::string out = get(a, "out", "");
+  const mesh::Mesh m = makeMesh(dim, n, n, n, 1.0, 1.0, 1.0);
+  const Index cells = m.numberOfCells();
+
+  boundary::BoundaryConditionSet pBCs;
+  for (const auto& patch : m.boundaryPatches())
+    pBCs.set(m, patch.name(), std::make_unique<boundary::FixedGradient>(0.0));
+  const fields::ScalarField one(cells, 1.0);
+  const fields::SurfaceField zeroFlux(m.numberOfFaces(), 0.0);
+  pressure_velocity::PressureCorrectionOptions opts;
+  auto assembly = pressure_velocity::assemblePressureCorrection(
+      m, zeroFlux, one, one, 1.0, 0, pBCs, opts, dim == 3 ? &one : nullptr);
+
+  std::vector<double> b(cells);
+  oracle_synth_rhs(n, n, dim == 3 ? n : 0, seed, b.data());
+  algebra::Vector rhs(cells);
+  for (Index i = 0; i < cells; ++i) rhs[i] = b[i];
+  const algebra::LinearSystem system(algebra::SparseMatrix(assembly.system.matrix()), rhs);
+
+  algebra::LinearSolverSettings s;
+  s.absoluteTolerance = getd(a, "atol", 0.0);
+  s.relativeTolerance = getd(a, "rtol", 1e-8);
+  s.maxIterations = static_cast<Index>(geti(a, "maxit", 100000));
+  std::shared_ptr<algebra::Preconditioner> pre;
+  if (get(a, "pre", "jacobi") == "jacobi") pre = std::make_shared<algebra::JacobiPreconditioner>();
+  std::unique_ptr<algebra::LinearSolver> solver;
+  if (get(a, "solver", "cg") == "bicgstab")
+    solver = std::make_unique<algebra::BiCGSTAB>(s, pre);
+  else
+    solver = std::make_unique<algebra::CG>(s, pre);
+
+  const auto t0 = std::chrono::steady_clock::now();
+  const algebra::SolverResult r = solver->solve(system);
+  const auto t1 = std::chrono::steady_clock::now();
+  const double seconds = std::chrono::duration<double>(t1 - t0).count();
+
+  // FP64 true residual of the returned solution.
+  const algebra::Vector ax = system.matrix().multiply(r.solution);
+  double rr = 0.0, bb = 0.0;
+  for (Index i = 0; i < cells; ++i) {
+    const double d = rhs[i] - ax[i];
+    rr += d * d;
+    bb += rhs[i] * rhs[i];
+  }
+  std::printf(
+      "{\"status\": \"%s\", \"iterations\": %zu, \"initial_residual\": %.17g, "
+      "\"final_residual\": %.17g, \"true_rel_residual\": %.17g, \"seconds\": %.6f, "
+      "\"cells\": %zu, \"nnz\": %zu}\n",
+      solverStatusText(r.status), static_cast<size_t>(r.iterations), r.initialResidual,
+      r.finalResidual, std::sqrt(rr) / std::sqrt(bb), seconds, static_cast<size_t>(cells),
+      static_cast<size_t>(system.matrix().nonZeros()));
+  if (!out.empty()) {
+    writeBin(out + "/rhs.bin", b);
+    writeBin(out + "/x.bin", r.solution.data(), cells);
+    writeBin(out + "/hist.bin", r.residualHistory);
+    if (geti(a, "dump_matrix", 0) != 0) {
+      const auto& A = system.matrix();
+      std::vector<double> off(A.rows() + 1), col(A.nonZeros());
+      for (Index i = 0; i <= A.rows(); ++i) off[i] = static_cast<double>(A.rowOffsetsData()[i]);
+      for (Index k = 0; k < A.nonZeros(); ++k) col[k] = static_cast<double>(A.columnIndicesData()[k]);
+      writeBin(out + "/csr_offsets.bin", off);
+      writeBin(out + "/csr_columns.bin", col);
+      writeBin(out + "/csr_values.bin", A.valuesData(), A.nonZeros());
+    }
+  }
+  return 0;
+}
+
+algebra::LinearSolverSettings linSettings(const Args& a, const std::string& prefix,
+                                          const std::string& type, double abs, double rel,
+                                          long long maxit, const std::string& pre) {
+  algebra::LinearSolverSettings s;
+  s.absoluteTolerance = getd(a, prefix + "abs", abs);
+  s.relativeTolerance = getd(a, prefix + "rel", rel);
+  s.maxIterations = static_cast<Index>(geti(a, prefix + "max", maxit));
+  s.type = get(a, prefix + "solver", type) == "cg" ? algebra::LinearSolverType::CG
+                                                   : algebra::LinearSolverType::BiCGSTAB;
+  s.preconditioner = get(a, prefix + "pre", pre) == "jacobi" ? algebra::PreconditionerType::Jacobi
+                                                             : algebra::PreconditionerType::None;
+  return s;
+}
+
+int runSimple(const Args& a) {
+  const int dim = static_cast<int>(geti(a, "dim", 2));
+  const long long nx = geti(a, "nx", 16), ny = geti(a, "ny", nx), nz = geti(a, "nz", nx);
+  const double lx = getd(a, "lx", 1.0), ly = getd(a, "ly", 1.0), lz = getd(a, "lz", 1.0);
+  const std::string out = get(a, "out", "");
+  const std::string flow = get(a, "flow", "cavity");
+  const mesh::Mesh m = makeMesh(dim, nx, ny, nz, lx, ly, lz);
+  const Index cells = m.numberOfCells();
+  const physics::FluidProperties fluid(getd(a, "rho", 1.0), getd(a, "mu", 0.01));
+
+  boundary::BoundaryConditionSet vBCs, pBCs;
+  const double lid = getd(a, "lid", 1.0), inlet = getd(a, "inlet", 1.0);
+  for (const auto& patch : m.boundaryPatches()) {
+    const std::string& name = patch.name();
+    if (flow == "channel" && (name == "left" || name == "xmin")) {
+      vBCs.set(m, name, std::make_unique<boundary::Inlet>(Vector2{inlet, 0.0}));
+      pBCs.set(m, name, std::make_unique<boundary::FixedGradient>(0.0));
+    } else if (flow == "channel" && (name == "right" || name == "xmax")) {
+      vBCs.set(m, name, std::make_unique<boundary::Outlet>());
+      pBCs.set(m, name, std::make_unique<boundary::FixedValue>(0.0));
+    } else if (flow == "cavity" && (name == "top" || name == "ymax")) {
+      vBCs.set(m, name, std::make_unique<boundary::MovingWall>(Vector2{lid, 0.0}));
+      pBCs.set(m, name, std::make_unique<boundary::FixedGradient>(0.0));
+    } else {
+      vBCs.set(m, name, std::make_unique<boundary::Wall>());
+      pBCs.set(m, name, std::make_unique<boundary::FixedGradient>(0.0));
+    }
+  }
+
+  pressure_velocity::SIMPLESettings s;
+  s.maxIterations = static_cast<Index>(geti(a, "outer", 1000));
+  s.velocityRelaxation = getd(a, "au", 0.7);
+  s.pressureRelaxation = getd(a, "ap", 0.3);
+  s.velocityTolerance = getd(a, "tolu", 1e-6);
+  s.pressureTolerance = getd(a, "tolp", 1e-6);
+  s.continuityTolerance = getd(a, "tolc", 1e-6);
+  s.momentumSolver = linSettings(a, "m", "bicgstab", 1e-10, 1e-8, 500, "none");
+  s.pressureSolver = linSettings(a, "p", "cg", 0.0, 1e-8, 5000, "jacobi");
+  const std::string scheme = get(a, "scheme", "upwind");
+  s.convectionScheme = scheme == "central" ? discretization::ConvectionScheme::Central
+                       : scheme == "lud"   ? discretization::ConvectionScheme::LinearUpwind
+                       : scheme == "quick" ? discretization::ConvectionScheme::QUICK
+                                           : discretization::ConvectionScheme::Upwind;
+  const std::string flux = get(a, "flux", "auto");
+  s.faceFlux = flux == "linear"     ? pressure_velocity::FaceFluxScheme::Linear
+               : flux == "rhiechow" ? pressure_velocity::FaceFluxScheme::RhieChow
+                                    : pressure_velocity::FaceFluxScheme::Automatic;
+
+  fields::VectorField U0(cells, Vector2{0.0, 0.0});
+  fields::ScalarField p0(cells, 0.0);
+  const pressure_velocity::SIMPLE simple(s, 0);
+  const auto t0 = std::chrono::steady_clock::now();
+  const auto r = simple.solve(m, fluid, vBCs, pBCs, U0, p0);
+  const double seconds =
+      std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+
+  std::printf(
+      "{\"status\": \"%s\", \"iterations\": %zu, \"final_u\": %.17g, \"final_v\": %.17g, "
+      "\"final_w\": %.17g, \"final_p\": %.17g, \"final_continuity\": %.17g, "
+      "\"global_imbalance\": %.17g, \"momentum_linear_iterations\": %zu, "
+      "\"pressure_linear_iterations\": %zu, \"seconds\": %.6f, \"pressure_solve_seconds\": %.6f, "
+      "\"momentum_assembly_seconds\": %.6f, \"momentum_solve_seconds\": %.6f, "
+      "\"pressure_assembly_seconds\": %.6f, \"cells\": %zu, \"faces\": %zu}\n",
+      simpleStatusName(r.status), static_cast<size_t>(r.iterations), r.finalUResidual,
+      r.finalVResidual, r.finalWResidual, r.finalPressureResidual, r.finalContinuityResidual,
+      r.globalMassImbalance, static_cast<size_t>(r.momentumLinearIterations),
+      static_cast<size_t>(r.pressureLinearIterations), seconds, r.stageSeconds.pressureSolve,
+      r.stageSeconds.momentumAssembly, r.stageSeconds.momentumSolve,
+      r.stageSeconds.pressureAssembly, static_cast<size_t>(cells),
+      static_cast<size_t>(m.numberOfFaces()));
+  if (!out.empty()) {
+    std::vector<double> u(cells), v(cells), w(cells), p(cells);
+    for (Index i = 0; i < cells; ++i) {
+      u[i] = r.velocity[i].x;
+      v[i] = r.velocity[i].y;
+      w[i] = r.velocity[i].z;
+      p[i] = r.pressure[i];
+    }
+    writeBin(out + "/u.bin", u);
+    writeBin(out + "/v.bin", v);
+    if (dim == 3) writeBin(out + "/w.bin", w);
+    writeBin(out + "/p.bin", p);
+    writeBin(out + "/flux.bin", r.massFlux.data(), r.massFlux.size());
+    std::vector<double> hist;
+    for (size_t k = 0; k < r.uResidualHistory.size(); ++k) {
+      hist.push_back(r.uResidualHistory[k]);
+      hist.push_back(r.vResidualHistory[k]);
+      hist.push_back(dim == 3 ? r.wResidualHistory[k] : 0.0);
+      hist.push_back(r.pressureResidualHistory[k]);
+      hist.push_back(r.continuityHistory[k]);
+    }
+    writeBin(out + "/hist.bin", hist);
+  }
+  return 0;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+  if (argc < 2) {
+    std::fprintf(stderr, "usage: ref_driver poisson|simple key=value ...\n");
+    return 2;
+  }
+  Args a;
+  for (int i = 2; i < argc; ++i) {
+    const std::string kv = argv[i];
+    const auto eq = kv.find('=');
+    if (eq == std::string::npos) {
+      std::fprintf(stderr, "bad argument %s\n", argv[i]);
+      return 2;
+    }
+    a[kv.substr(0, eq)] = kv.substr(eq + 1);
+  }
+  const std::string cmd = argv[1];
+  try {
+    if (cmd == "poisson") return runPoisson(a);
+    if (cmd == "simple") return runSimple(a);
+  } catch (const std::exception& e) {
+    std::fprintf(stderr, "ref_driver: %s\n", e.what());
+    return 1;
+  }
+  std::fprintf(stderr, "unknown command %s\n", cmd.c_str());
+  return 2;
+}
