@@ -1,0 +1,901 @@
+// p' operator objects and their Krylov solves.
+//
+// The plain method is the reference's Jacobi-preconditioned CG
+// (src/algebra/CG.cpp:14-148, JacobiPreconditioner src/algebra/Preconditioner.cpp:11-49)
+// with its exact status and convergence semantics, run as ONE persistent
+// cooperative kernel per solve: two fused sweeps per iteration
+//   sweep A: p = D^-1 r + beta p_old (computed on the fly, halo included),
+//            Ap = A p, partial p.Ap, store p
+//   sweep B: x += alpha p, r -= alpha A p (A p recomputed from p),
+//            partial r.r and r.z (z = D^-1 r)
+// separated by bounded grid barriers; every block derives alpha/beta from the
+// same fixed-order sum of the per-block partials, so the whole solve runs on
+// the device with no host round trip (the reference synchronises and sums on
+// the host once per reduction, DeviceVectorOpsKernel.cu:226-260).
+//
+// The FP32-refined method runs the same kernel in FP32 (FP64 reductions)
+// inside FP64 iterative refinement: r = b - A x in FP64 (fused with the update
+// x += e), inner PCG on A e = r in FP32 to a moderate reduction, repeat until
+// the FP64 true residual meets the tolerance.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "cfdb.h"
+#include "cfdb_internal.cuh"
+#include "grid_sync.cuh"
+#include "poperator.cuh"
+
+struct cfdb_poperator {
+  cfdb_context* ctx = nullptr;
+  cfdb_grid grid{};
+  int knx = 0, kny = 0, knz = 0;  // kernel-space extents
+  int64_t cells = 0;
+  int pinned = 0;
+  int64_t ref = 0;
+  // FP64 and FP32 copies of the coefficients (tables always; faces optional)
+  double* t64[3] = {nullptr, nullptr, nullptr};
+  float* t32[3] = {nullptr, nullptr, nullptr};
+  double* f64[3] = {nullptr, nullptr, nullptr};
+  float* f32[3] = {nullptr, nullptr, nullptr};
+  // work vectors, allocated on first solve
+  double* w64[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};  // r p0 p1 xalt b x (host staging)
+  float* w32[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};   // r p0 p1 e b32
+  double* hist_dev = nullptr;
+  int64_t hist_cap = 0;
+};
+
+namespace cfdb {
+namespace {
+
+constexpr int kThreads = 256;
+constexpr unsigned long long kBarrierTimeoutNs = 2000000000ull;  // 2 s per barrier wait
+
+enum { OUT_STATUS = 0, OUT_ITER = 1, OUT_B0 = 2, OUT_FINAL = 3, OUT_PCUR = 4, OUT_TIMEOUT = 5 };
+
+template <typename T>
+OpView<T> view(const cfdb_poperator* op) {
+  OpView<T> v;
+  v.nx = op->knx;
+  v.ny = op->kny;
+  v.nz = op->knz;
+  if constexpr (sizeof(T) == 8) {
+    v.tx = op->t64[0]; v.ty = op->t64[1]; v.tz = op->t64[2];
+    v.fx = op->f64[0]; v.fy = op->f64[1]; v.fz = op->f64[2];
+  } else {
+    v.tx = op->t32[0]; v.ty = op->t32[1]; v.tz = op->t32[2];
+    v.fx = op->f32[0]; v.fy = op->f32[1]; v.fz = op->f32[2];
+  }
+  v.ref = op->ref;
+  v.pinned = op->pinned;
+  return v;
+}
+
+template <typename T>
+struct PcgParams {
+  OpView<T> A;
+  Tiling tl;
+  const T* b;
+  T* x;
+  T* r;
+  T* p0;
+  T* p1;
+  int x0_zero;
+  double abs_tol, rel_tol;
+  int64_t max_it;
+  double* hist;
+  int64_t hist_cap;
+  double* partials;
+  GridSync sync;
+  double* out;
+};
+
+__device__ __forceinline__ bool finite(double v) { return isfinite(v); }
+
+template <typename T, int PY>
+__global__ void __launch_bounds__(kThreads, 3) pcg_persistent(PcgParams<T> P) {
+  constexpr int PX = kThreads / PY;
+  __shared__ T buf[2][PY + 2][PX + 2];
+  __shared__ double red[64];
+  const OpView<T>& A = P.A;
+  const int B = gridDim.x, blk = blockIdx.x;
+  const bool leader = (blockIdx.x == 0 && threadIdx.x == 0 && threadIdx.y == 0);
+  // Partials are double-buffered by reduction round: a block that already
+  // summed round k and raced ahead writes round k+1 into the other half while
+  // slower blocks may still be reading round k.
+  int round = 0;
+  auto part = [&]() { return P.partials + (size_t)(round & 1) * 2 * B; };
+
+  // ---- r0 = b - A x0, ||r0||^2, r0.z0
+  double acc[2] = {0.0, 0.0};
+  for_segments(P.tl, A.nz, blk, B, [&](int64_t tile, int k0, int k1) {
+    march<T, PX, PY>(
+        A, P.tl, tile, k0, k1, buf,
+        [&](int i, int j, int k) {
+          const int64_t idx = i + (int64_t)A.nx * (j + (int64_t)A.ny * k);
+          return P.x0_zero ? T(0) : P.x[idx];
+        },
+        [&](int i, int j, int k) {
+          const int64_t idx = i + (int64_t)A.nx * (j + (int64_t)A.ny * k);
+          return P.x0_zero ? T(0) : P.x[idx];
+        },
+        [&](int i, int j, int k, int64_t idx, T v, T w, T e, T s, T n, T bb, T t) {
+          const Coef<T> c = load_coef(A, i, j, k);
+          T rn = __ldg(P.b + idx);
+          if (!P.x0_zero) rn = rn - apply_coef(c, v, w, e, s, n, bb, t);
+          P.r[idx] = rn;
+          const double rd = (double)rn;
+          acc[0] += rd * rd;
+          acc[1] += rd * (double)(c.inv * rn);
+        });
+  });
+  block_sum<2>(acc, red);
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    part()[2 * blk] = acc[0];
+    part()[2 * blk + 1] = acc[1];
+  }
+  if (!grid_sync(P.sync)) return;
+  double tot[2];
+  grid_total<2>(part(), 2, B, tot, red);
+  ++round;
+  const double b0 = sqrt(tot[0]);
+  double rz = tot[1];
+  auto converged = [&](double res) {
+    return (res <= P.abs_tol) || ((b0 > 0.0) && (res / b0 <= P.rel_tol));
+  };
+  if (leader) {
+    P.out[OUT_B0] = b0;
+    if (P.hist_cap > 0) P.hist[0] = b0;
+  }
+  if (b0 == 0.0 || converged(b0)) {
+    if (leader) {
+      P.out[OUT_STATUS] = CFDB_SOLVER_CONVERGED;
+      P.out[OUT_ITER] = 0;
+      P.out[OUT_FINAL] = b0;
+    }
+    return;
+  }
+  if (!finite(rz)) {
+    if (leader) {
+      P.out[OUT_STATUS] = CFDB_SOLVER_BREAKDOWN;
+      P.out[OUT_ITER] = 0;
+      P.out[OUT_FINAL] = b0;
+    }
+    return;
+  }
+
+  double res_cur = b0;
+  double beta = 0.0;
+  T* pold = P.p0;
+  T* pnew = P.p1;
+  for (int64_t it = 1; it <= P.max_it; ++it) {
+    const bool first = (it == 1);
+    const T tbeta = (T)beta;
+    // ---- sweep A: p = z + beta p_old; Ap; p.Ap
+    double pap = 0.0;
+    auto pz = [&](int i, int j, int k) {
+      const Coef<T> c = load_coef(A, i, j, k);
+      const int64_t idx = i + (int64_t)A.nx * (j + (int64_t)A.ny * k);
+      const T z = c.inv * __ldcg(P.r + idx);
+      return first ? z : fma(tbeta, __ldcg(pold + idx), z);
+    };
+    for_segments(P.tl, A.nz, blk, B, [&](int64_t tile, int k0, int k1) {
+      march<T, PX, PY>(
+          A, P.tl, tile, k0, k1, buf,
+          pz, pz,
+          [&](int i, int j, int k, int64_t idx, T v, T w, T e, T s, T n, T bb, T t) {
+            const Coef<T> c = load_coef(A, i, j, k);
+            const T ap = apply_coef(c, v, w, e, s, n, bb, t);
+            pnew[idx] = v;
+            pap += (double)v * (double)ap;
+          });
+    });
+    {
+      double a1[1] = {pap};
+      block_sum<1>(a1, red);
+      if (threadIdx.x == 0 && threadIdx.y == 0) part()[2 * blk] = a1[0];
+    }
+    if (!grid_sync(P.sync)) return;
+    double t1[1];
+    grid_total<1>(part(), 2, B, t1, red);
+    ++round;
+    const double pAp = t1[0];
+    const double alpha = rz / pAp;
+    if (!finite(pAp) || fabs(pAp) < 1.0e-30 || !finite(alpha)) {
+      if (leader) {
+        P.out[OUT_STATUS] = CFDB_SOLVER_BREAKDOWN;
+        P.out[OUT_ITER] = (double)(it - 1);
+        P.out[OUT_FINAL] = res_cur;
+      }
+      return;
+    }
+    const T talpha = (T)alpha;
+    // ---- sweep B: x += alpha p; r -= alpha A p; r.r, r.z
+    double ab[2] = {0.0, 0.0};
+    for_segments(P.tl, A.nz, blk, B, [&](int64_t tile, int k0, int k1) {
+      march<T, PX, PY>(
+          A, P.tl, tile, k0, k1, buf,
+          [&](int i, int j, int k) {
+            return __ldcg(pnew + (i + (int64_t)A.nx * (j + (int64_t)A.ny * k)));
+          },
+          [&](int i, int j, int k) {
+            return __ldcg(pnew + (i + (int64_t)A.nx * (j + (int64_t)A.ny * k)));
+          },
+          [&](int i, int j, int k, int64_t idx, T v, T w, T e, T s, T n, T bb, T t) {
+            const Coef<T> c = load_coef(A, i, j, k);
+            const T ap = apply_coef(c, v, w, e, s, n, bb, t);
+            P.x[idx] = fma(talpha, v, P.x[idx]);
+            const T rn = fma(-talpha, ap, __ldcg(P.r + idx));
+            P.r[idx] = rn;
+            const double rd = (double)rn;
+            ab[0] += rd * rd;
+            ab[1] += rd * (double)(c.inv * rn);
+          });
+    });
+    block_sum<2>(ab, red);
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+      part()[2 * blk] = ab[0];
+      part()[2 * blk + 1] = ab[1];
+    }
+    if (!grid_sync(P.sync)) return;
+    grid_total<2>(part(), 2, B, tot, red);
+    ++round;
+    const double res = sqrt(tot[0]);
+    if (leader && it < P.hist_cap) P.hist[it] = res;
+    if (!finite(res)) {
+      if (leader) {
+        P.out[OUT_STATUS] = CFDB_SOLVER_NONFINITE_RESIDUAL;
+        P.out[OUT_ITER] = (double)it;
+        P.out[OUT_FINAL] = res;
+      }
+      return;
+    }
+    res_cur = res;
+    if (converged(res)) {
+      if (leader) {
+        P.out[OUT_STATUS] = CFDB_SOLVER_CONVERGED;
+        P.out[OUT_ITER] = (double)it;
+        P.out[OUT_FINAL] = res;
+      }
+      return;
+    }
+    const double rzNew = tot[1];
+    beta = rzNew / rz;
+    if (!finite(rzNew) || !finite(beta)) {
+      if (leader) {
+        P.out[OUT_STATUS] = CFDB_SOLVER_BREAKDOWN;
+        P.out[OUT_ITER] = (double)it;
+        P.out[OUT_FINAL] = res;
+      }
+      return;
+    }
+    rz = rzNew;
+    T* tmp = pold;
+    pold = pnew;
+    pnew = tmp;
+    if (leader) P.out[OUT_ITER] = (double)it;
+  }
+  if (leader) {
+    P.out[OUT_STATUS] = CFDB_SOLVER_MAX_ITERATIONS;
+    P.out[OUT_ITER] = (double)P.max_it;
+    P.out[OUT_FINAL] = res_cur;
+  }
+}
+
+// FP64 residual pass of the refinement: x_out = x_in + scale * e (e may be
+// null), r = b - A x_out; optionally r32 = (float) r; per-block ||r||^2.
+template <int PY>
+__global__ void __launch_bounds__(kThreads) refine_residual(OpView<double> A, Tiling tl,
+                                                            const double* b, const double* x_in,
+                                                            double* x_out, const float* e,
+                                                            double scale, float* r32,
+                                                            double* r64, double* partials) {
+  constexpr int PX = kThreads / PY;
+  __shared__ double buf[2][PY + 2][PX + 2];
+  __shared__ double red[64];
+  double acc[1] = {0.0};
+  auto value = [&](int i, int j, int k) {
+    const int64_t idx = i + (int64_t)A.nx * (j + (int64_t)A.ny * k);
+    double v = __ldg(x_in + idx);
+    if (e) v = fma(scale, (double)__ldg(e + idx), v);
+    return v;
+  };
+  for_segments(tl, A.nz, blockIdx.x, gridDim.x, [&](int64_t tile, int k0, int k1) {
+    march<double, PX, PY>(
+        A, tl, tile, k0, k1, buf,
+        value, value,
+        [&](int i, int j, int k, int64_t idx, double v, double w, double ee, double s, double n,
+            double bb, double t) {
+          const Coef<double> c = load_coef(A, i, j, k);
+          if (x_out) x_out[idx] = v;
+          const double rn = __ldg(b + idx) - apply_coef(c, v, w, ee, s, n, bb, t);
+          if (r32) r32[idx] = (float)rn;
+          if (r64) r64[idx] = rn;
+          acc[0] += rn * rn;
+        });
+  });
+  block_sum<1>(acc, red);
+  if (threadIdx.x == 0 && threadIdx.y == 0) partials[blockIdx.x] = acc[0];
+}
+
+// One block: out[slot] = sum of partials[0..n) in fixed order.
+__global__ void sum_partials(const double* partials, int n, double* out, int slot) {
+  __shared__ double red[64];
+  double a[1] = {0.0};
+  for (int q = threadIdx.x; q < n; q += blockDim.x) a[0] += partials[q];
+  block_sum<1>(a, red);
+  if (threadIdx.x == 0) out[slot] = a[0];
+}
+
+// y = A x (FP64).
+template <int PY>
+__global__ void __launch_bounds__(kThreads) apply_kernel(OpView<double> A, Tiling tl,
+                                                         const double* x, double* y) {
+  constexpr int PX = kThreads / PY;
+  __shared__ double buf[2][PY + 2][PX + 2];
+  auto value = [&](int i, int j, int k) {
+    return __ldg(x + (i + (int64_t)A.nx * (j + (int64_t)A.ny * k)));
+  };
+  for_segments(tl, A.nz, blockIdx.x, gridDim.x, [&](int64_t tile, int k0, int k1) {
+    march<double, PX, PY>(
+        A, tl, tile, k0, k1, buf,
+        value, value,
+        [&](int i, int j, int k, int64_t idx, double v, double w, double e, double s, double n,
+            double bb, double t) {
+          const Coef<double> c = load_coef(A, i, j, k);
+          y[idx] = apply_coef(c, v, w, e, s, n, bb, t);
+        });
+  });
+}
+
+__global__ void all_finite(const double* v, int64_t n, unsigned* flag) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n;
+       q += (int64_t)gridDim.x * blockDim.x)
+    if (!isfinite(v[q])) atomicExch(flag, 1u);
+}
+
+// ------------------------------------------------------------------ host side
+
+bool is3d(const cfdb_poperator* op) { return op->grid.dim == 3; }
+
+template <typename T, int PY>
+cfdb_status launch_pcg(cfdb_context* ctx, PcgParams<T>& P) {
+  auto kernel = pcg_persistent<T, PY>;
+  int per_sm = 0;
+  CFDB_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel,
+                                                                kThreads, 0));
+  if (per_sm < 1) return set_error(ctx, CFDB_ERR_CUDA, "pcg kernel cannot be resident");
+  int64_t grid = (int64_t)per_sm * ctx->num_sms;
+  grid = std::min<int64_t>(grid, P.tl.items);
+  grid = std::max<int64_t>(grid, 1);
+  cfdb_status st = ensure_partials(ctx, 4 * (size_t)grid);
+  if (st != CFDB_OK) return st;
+  P.partials = ctx->partials;
+  P.sync.count = ctx->sync_words;
+  P.sync.gen = ctx->sync_words + 1;
+  P.sync.error = ctx->sync_words + 2;
+  P.sync.nblocks = (unsigned)grid;
+  P.sync.timeout_ns = kBarrierTimeoutNs;
+  P.out = ctx->scalars;
+  CFDB_CUDA(ctx, cudaMemsetAsync(ctx->sync_words, 0, 4 * sizeof(unsigned), ctx->stream));
+  CFDB_CUDA(ctx, cudaMemsetAsync(ctx->scalars, 0, 8 * sizeof(double), ctx->stream));
+  dim3 block(kThreads / PY, PY);
+  void* args[] = {&P};
+  CFDB_CUDA(ctx, cudaEventRecord(ctx->ev_k0, ctx->stream));
+  CFDB_CUDA(ctx, cudaLaunchCooperativeKernel((const void*)kernel, dim3((unsigned)grid), block, args,
+                                             0, ctx->stream));
+  CFDB_CUDA(ctx, cudaEventRecord(ctx->ev_k1, ctx->stream));
+  count_launch(ctx);
+  return CFDB_OK;
+}
+
+template <typename T>
+cfdb_status run_pcg(cfdb_context* ctx, const cfdb_poperator* op, const T* b, T* x, T* r, T* p0,
+                    T* p1, int x0_zero, double abs_tol, double rel_tol, int64_t max_it,
+                    double* hist_dev, int64_t hist_cap) {
+  PcgParams<T> P{};
+  P.A = view<T>(op);
+  P.b = b;
+  P.x = x;
+  P.r = r;
+  P.p0 = p0;
+  P.p1 = p1;
+  P.x0_zero = x0_zero;
+  P.abs_tol = abs_tol;
+  P.rel_tol = rel_tol;
+  P.max_it = max_it;
+  P.hist = hist_dev;
+  P.hist_cap = hist_cap;
+  if (is3d(op)) {
+    P.tl = make_tiling<32, 8>(op->knx, op->kny, op->knz);
+    return launch_pcg<T, 8>(ctx, P);
+  }
+  P.tl = make_tiling<256, 1>(op->knx, op->kny, op->knz);
+  return launch_pcg<T, 1>(ctx, P);
+}
+
+// Algorithmic bytes of one persistent PCG launch: the initial pass reads b
+// (and x0) and writes r; each iteration moves 8 vector words per cell (sweep
+// A: r, p_old in, p out; sweep B: x, r, p in, x, r out) plus, with per-face
+// coefficients, the face words each sweep reads.
+double pcg_bytes(const cfdb_poperator* op, size_t word, int64_t iterations, bool x0_zero) {
+  const double cells = (double)op->cells;
+  int face_words = 0;
+  for (int q = 0; q < 3; ++q) face_words += op->f64[q] ? 1 : 0;
+  const double init = cells * (x0_zero ? 2.0 : 3.0) * (double)word;
+  const double per_it = cells * (8.0 + 2.0 * face_words) * (double)word;
+  return init + per_it * (double)iterations;
+}
+
+cfdb_status add_krylov_time(cfdb_context* ctx, cfdb_linear_result* res) {
+  float ms = 0.f;
+  CFDB_CUDA(ctx, cudaEventElapsedTime(&ms, ctx->ev_k0, ctx->ev_k1));
+  res->krylov_ms += ms;
+  res->krylov_launches += 1;
+  return CFDB_OK;
+}
+
+// Reads the solver scalars back (one small synchronous copy).
+cfdb_status read_scalars(cfdb_context* ctx, int n) {
+  CFDB_CUDA(ctx, cudaMemcpyAsync(ctx->scalars_host, ctx->scalars, n * sizeof(double),
+                                 cudaMemcpyDeviceToHost, ctx->stream));
+  unsigned err = 0;
+  CFDB_CUDA(ctx, cudaMemcpyAsync(&err, ctx->sync_words + 2, sizeof(unsigned),
+                                 cudaMemcpyDeviceToHost, ctx->stream));
+  CFDB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (err != 0)
+    return set_error(ctx, CFDB_ERR_DEVICE_TIMEOUT,
+                     "a grid barrier of the persistent solver timed out (no fault; solve abandoned)");
+  return CFDB_OK;
+}
+
+// FP64 ||b - A x_in - scale e|| with optional outputs; returns the norm.
+cfdb_status refine_pass(cfdb_context* ctx, const cfdb_poperator* op, const double* b,
+                        const double* x_in, double* x_out, const float* e, double scale,
+                        float* r32, double* r64, double* norm_out) {
+  const OpView<double> A = view<double>(op);
+  Tiling tl;
+  int grid;
+  const int chunk = 16;
+  if (is3d(op)) {
+    tl = make_tiling<32, 8>(op->knx, op->kny, op->knz);
+  } else {
+    tl = make_tiling<256, 1>(op->knx, op->kny, op->knz);
+  }
+  grid = (int)std::max<int64_t>(1, std::min<int64_t>((tl.items + chunk - 1) / chunk, 1 << 20));
+  cfdb_status st = ensure_partials(ctx, grid);
+  if (st != CFDB_OK) return st;
+  if (is3d(op))
+    refine_residual<8><<<grid, dim3(32, 8), 0, ctx->stream>>>(A, tl, b, x_in, x_out, e, scale, r32,
+                                                              r64, ctx->partials);
+  else
+    refine_residual<1><<<grid, dim3(256, 1), 0, ctx->stream>>>(A, tl, b, x_in, x_out, e, scale,
+                                                               r32, r64, ctx->partials);
+  CFDB_CHECK_LAUNCH(ctx);
+  sum_partials<<<1, 256, 0, ctx->stream>>>(ctx->partials, grid, ctx->scalars, 8);
+  CFDB_CHECK_LAUNCH(ctx);
+  count_launch(ctx, 2);
+  CFDB_CUDA(ctx, cudaMemcpyAsync(ctx->scalars_host + 8, ctx->scalars + 8, sizeof(double),
+                                 cudaMemcpyDeviceToHost, ctx->stream));
+  CFDB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  *norm_out = std::sqrt(ctx->scalars_host[8]);
+  return CFDB_OK;
+}
+
+template <typename T>
+cfdb_status alloc_vec(cfdb_context* ctx, T** p, int64_t n) {
+  if (*p) return CFDB_OK;
+  CFDB_CUDA(ctx, cudaMalloc((void**)p, sizeof(T) * (size_t)n));
+  return CFDB_OK;
+}
+
+cfdb_status ensure_hist(cfdb_context* ctx, cfdb_poperator* op, int64_t cap) {
+  if (op->hist_cap >= cap && op->hist_dev) return CFDB_OK;
+  if (op->hist_dev) cudaFree(op->hist_dev);
+  op->hist_dev = nullptr;
+  op->hist_cap = 0;
+  CFDB_CUDA(ctx, cudaMalloc((void**)&op->hist_dev, sizeof(double) * (size_t)cap));
+  op->hist_cap = cap;
+  return CFDB_OK;
+}
+
+cfdb_status check_finite(cfdb_context* ctx, const double* v, int64_t n, bool* ok) {
+  CFDB_CUDA(ctx, cudaMemsetAsync(ctx->sync_words + 3, 0, sizeof(unsigned), ctx->stream));
+  const int grid = (int)std::min<int64_t>((n + 255) / 256, 4 * 148 * 8);
+  all_finite<<<std::max(grid, 1), 256, 0, ctx->stream>>>(v, n, ctx->sync_words + 3);
+  CFDB_CHECK_LAUNCH(ctx);
+  count_launch(ctx);
+  unsigned flag = 0;
+  CFDB_CUDA(ctx, cudaMemcpyAsync(&flag, ctx->sync_words + 3, sizeof(unsigned),
+                                 cudaMemcpyDeviceToHost, ctx->stream));
+  CFDB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  *ok = (flag == 0);
+  return CFDB_OK;
+}
+
+// Plain FP64 PCG on device vectors.
+cfdb_status solve_fp64(cfdb_context* ctx, cfdb_poperator* op, const cfdb_linear_settings* s,
+                       const double* b, double* x, bool x0_zero, int64_t hist_cap,
+                       cfdb_linear_result* res) {
+  const int64_t n = op->cells;
+  for (int q = 0; q < 3; ++q) {
+    cfdb_status st = alloc_vec(ctx, &op->w64[q], n);
+    if (st != CFDB_OK) return st;
+  }
+  cfdb_status st = ensure_hist(ctx, op, std::max<int64_t>(hist_cap, 1));
+  if (st != CFDB_OK) return st;
+  st = run_pcg<double>(ctx, op, b, x, op->w64[0], op->w64[1], op->w64[2], x0_zero ? 1 : 0,
+                       s->abs_tol, s->rel_tol, s->max_iterations, op->hist_dev, hist_cap);
+  if (st != CFDB_OK) return st;
+  st = read_scalars(ctx, 8);
+  if (st != CFDB_OK) return st;
+  const double* o = ctx->scalars_host;
+  res->status = (int)o[OUT_STATUS];
+  res->iterations = (int64_t)o[OUT_ITER];
+  res->initial_residual = o[OUT_B0];
+  res->final_residual = o[OUT_FINAL];
+  res->krylov_bytes += pcg_bytes(op, sizeof(double), res->iterations, x0_zero);
+  return add_krylov_time(ctx, res);
+}
+
+// FP32 inner sweeps inside FP64 iterative refinement.
+cfdb_status solve_refined(cfdb_context* ctx, cfdb_poperator* op, const cfdb_linear_settings* s,
+                          const double* b, double* x, int64_t hist_cap, double* hist_host,
+                          cfdb_linear_result* res) {
+  const int64_t n = op->cells;
+  for (int q = 0; q < 5; ++q) {
+    cfdb_status st = alloc_vec(ctx, &op->w32[q], n);
+    if (st != CFDB_OK) return st;
+  }
+  cfdb_status st = alloc_vec(ctx, &op->w64[3], n);
+  if (st != CFDB_OK) return st;
+  st = ensure_hist(ctx, op, 2);
+  if (st != CFDB_OK) return st;
+  const double inner_tol = s->inner_rel_tol > 0.0 ? s->inner_rel_tol : 1.0e-4;
+  const int64_t max_ref = s->max_refinements > 0 ? s->max_refinements : 50;
+  float* r32 = op->w32[0];
+  float* e32 = op->w32[3];
+  float* b32 = op->w32[4];
+  double* xa = x;
+  double* xb = op->w64[3];
+  // r = b - A x0 (FP64), r32 = float(r)
+  double rnorm = 0.0;
+  st = refine_pass(ctx, op, b, xa, nullptr, nullptr, 0.0, b32, nullptr, &rnorm);
+  if (st != CFDB_OK) return st;
+  const double b0 = rnorm;
+  res->initial_residual = b0;
+  int64_t hc = 0;
+  if (hist_host && hc < hist_cap) hist_host[hc] = b0;
+  ++hc;
+  auto conv = [&](double r) { return r <= s->abs_tol || (b0 > 0.0 && r / b0 <= s->rel_tol); };
+  int64_t inner_total = 0, steps = 0;
+  res->status = CFDB_SOLVER_MAX_ITERATIONS;
+  if (!std::isfinite(b0)) {
+    res->status = CFDB_SOLVER_NONFINITE_RESIDUAL;
+    res->final_residual = b0;
+    return CFDB_OK;
+  }
+  if (b0 == 0.0 || conv(b0)) {
+    res->status = CFDB_SOLVER_CONVERGED;
+    res->final_residual = b0;
+    return CFDB_OK;
+  }
+  while (steps < max_ref && inner_total < s->max_iterations) {
+    // inner: A e = r32 from e = 0 in FP32, reduction inner_tol
+    const int64_t budget = s->max_iterations - inner_total;
+    CFDB_CUDA(ctx, cudaMemsetAsync(e32, 0, sizeof(float) * (size_t)n, ctx->stream));
+    st = run_pcg<float>(ctx, op, b32, e32, r32, op->w32[1], op->w32[2], 1, 0.0, inner_tol,
+                        budget, op->hist_dev, 0);
+    if (st != CFDB_OK) return st;
+    st = read_scalars(ctx, 8);
+    if (st != CFDB_OK) return st;
+    const double* o = ctx->scalars_host;
+    const int inner_status = (int)o[OUT_STATUS];
+    inner_total += (int64_t)o[OUT_ITER];
+    res->krylov_bytes += pcg_bytes(op, sizeof(float), (int64_t)o[OUT_ITER], true);
+    st = add_krylov_time(ctx, res);
+    if (st != CFDB_OK) return st;
+    ++steps;
+    // x += e; r = b - A x (FP64); r32 = float(r)
+    st = refine_pass(ctx, op, b, xa, xb, e32, 1.0, b32, nullptr, &rnorm);
+    if (st != CFDB_OK) return st;
+    std::swap(xa, xb);
+    if (hist_host && hc < hist_cap) hist_host[hc] = rnorm;
+    ++hc;
+    if (!std::isfinite(rnorm)) {
+      res->status = CFDB_SOLVER_NONFINITE_RESIDUAL;
+      break;
+    }
+    if (conv(rnorm)) {
+      res->status = CFDB_SOLVER_CONVERGED;
+      break;
+    }
+    if (inner_status == CFDB_SOLVER_BREAKDOWN && (int64_t)o[OUT_ITER] == 0) {
+      res->status = CFDB_SOLVER_BREAKDOWN;
+      break;
+    }
+  }
+  if (xa != x) CFDB_CUDA(ctx, cudaMemcpyAsync(x, xa, sizeof(double) * n, cudaMemcpyDeviceToDevice,
+                                              ctx->stream));
+  res->final_residual = rnorm;
+  res->iterations = inner_total;
+  res->refinements = steps;
+  return CFDB_OK;
+}
+
+cfdb_status build_tables(cfdb_context* ctx, cfdb_poperator* op, double rho, unsigned dmask) {
+  // Geometry exactly as the reference evaluates it (MeshGrading.cpp
+  // AxisSpacing::uniform/center/node; MeshGeometry.cpp:513-552,1047-1140):
+  // D = ((rho * |S|) * d_face) / |x_N - x_P| with d_face = 1 (the scalar
+  // interpolation of a unit field is exactly 1), Dirichlet boundary faces
+  // ((rho * |S|) * 1) / |x_f - x_P|.
+  const cfdb_grid& g = op->grid;
+  const int dim = g.dim;
+  double delta[3] = {0, 0, 0};
+  for (int a = 0; a < dim; ++a) delta[a] = g.len[a] / (double)g.n[a];
+  double area[3] = {0, 0, 0};
+  if (dim == 2) {
+    area[0] = delta[1];
+    area[1] = delta[0];
+  } else {
+    area[0] = delta[1] * delta[2];
+    area[1] = delta[0] * delta[2];
+    area[2] = delta[0] * delta[1];
+  }
+  // real axis a -> kernel axis: 2D (x, y) -> (x, z); 3D identity
+  const int kaxis[3] = {0, dim == 2 ? 2 : 1, 2};
+  std::vector<double> tab[3];
+  tab[0].assign(op->knx + 1, 0.0);
+  tab[1].assign(op->kny + 1, 0.0);
+  tab[2].assign(op->knz + 1, 0.0);
+  for (int a = 0; a < dim; ++a) {
+    const int64_t n = g.n[a];
+    auto center = [&](int64_t i) { return ((double)i + 0.5) * delta[a]; };
+    auto node = [&](int64_t i) { return (double)i * delta[a]; };
+    std::vector<double>& t = tab[kaxis[a]];
+    for (int64_t f = 1; f < n; ++f) {
+      const double dPf = std::fabs(node(f) - center(f - 1));
+      const double dNf = std::fabs(node(f) - center(f));
+      const double dFace = ((dNf * 1.0) + (dPf * 1.0)) / (dPf + dNf);
+      const double dist = std::fabs(center(f) - center(f - 1));
+      t[f] = rho * area[a] * dFace / dist;
+    }
+    if (dmask & (1u << (2 * a))) t[0] = rho * area[a] * 1.0 / std::fabs(node(0) - center(0));
+    if (dmask & (1u << (2 * a + 1)))
+      t[n] = rho * area[a] * 1.0 / std::fabs(node(n) - center(n - 1));
+  }
+  for (int q = 0; q < 3; ++q) {
+    const size_t m = tab[q].size();
+    std::vector<float> t32(m);
+    for (size_t i = 0; i < m; ++i) t32[i] = (float)tab[q][i];
+    CFDB_CUDA(ctx, cudaMalloc((void**)&op->t64[q], m * sizeof(double)));
+    CFDB_CUDA(ctx, cudaMalloc((void**)&op->t32[q], m * sizeof(float)));
+    CFDB_CUDA(ctx, cudaMemcpy(op->t64[q], tab[q].data(), m * sizeof(double), cudaMemcpyHostToDevice));
+    CFDB_CUDA(ctx, cudaMemcpy(op->t32[q], t32.data(), m * sizeof(float), cudaMemcpyHostToDevice));
+  }
+  return CFDB_OK;
+}
+
+cfdb_status validate_grid(cfdb_context* ctx, const cfdb_grid* g) {
+  if (!g || (g->dim != 2 && g->dim != 3))
+    return set_error(ctx, CFDB_ERR_INVALID_ARGUMENT, "grid: dim must be 2 or 3");
+  for (int a = 0; a < g->dim; ++a) {
+    if (g->n[a] < 2 || g->n[a] > (1 << 20))
+      return set_error(ctx, CFDB_ERR_INVALID_ARGUMENT, "grid: each axis needs 2..2^20 cells");
+    if (!(g->len[a] > 0.0) || !std::isfinite(g->len[a]))
+      return set_error(ctx, CFDB_ERR_INVALID_ARGUMENT, "grid: lengths must be finite and > 0");
+  }
+  const int64_t cells = g->n[0] * g->n[1] * (g->dim == 3 ? g->n[2] : 1);
+  if (cells > ((int64_t)1 << 31))
+    return set_error(ctx, CFDB_ERR_INVALID_ARGUMENT, "grid: more than 2^31 cells");
+  return CFDB_OK;
+}
+
+cfdb_status new_operator(cfdb_context* ctx, const cfdb_grid* grid, int pinned, int64_t ref,
+                         cfdb_poperator** out) {
+  cfdb_status st = validate_grid(ctx, grid);
+  if (st != CFDB_OK) return st;
+  auto* op = new cfdb_poperator();
+  op->ctx = ctx;
+  op->grid = *grid;
+  op->knx = (int)grid->n[0];
+  if (grid->dim == 2) {
+    op->kny = 1;
+    op->knz = (int)grid->n[1];
+  } else {
+    op->kny = (int)grid->n[1];
+    op->knz = (int)grid->n[2];
+  }
+  op->cells = (int64_t)op->knx * op->kny * op->knz;
+  op->pinned = pinned ? 1 : 0;
+  op->ref = ref;
+  if (pinned && (ref < 0 || ref >= op->cells)) {
+    delete op;
+    return set_error(ctx, CFDB_ERR_INVALID_ARGUMENT, "reference cell out of range");
+  }
+  *out = op;
+  return CFDB_OK;
+}
+
+}  // namespace
+}  // namespace cfdb
+
+using namespace cfdb;
+
+extern "C" {
+
+cfdb_status cfdb_poperator_create_uniform(cfdb_context* ctx, const cfdb_grid* grid, double rho,
+                                          unsigned dirichlet_patch_mask, int pinned,
+                                          int64_t reference_cell, cfdb_poperator** out) {
+  if (!ctx || !out) return CFDB_ERR_INVALID_ARGUMENT;
+  if (!(rho > 0.0) || !std::isfinite(rho))
+    return set_error(ctx, CFDB_ERR_INVALID_ARGUMENT, "density must be finite and > 0");
+  CFDB_CUDA(ctx, cudaSetDevice(ctx->device));
+  cfdb_poperator* op = nullptr;
+  cfdb_status st = new_operator(ctx, grid, pinned, reference_cell, &op);
+  if (st != CFDB_OK) return st;
+  st = build_tables(ctx, op, rho, dirichlet_patch_mask);
+  if (st != CFDB_OK) {
+    cfdb_poperator_destroy(op);
+    return st;
+  }
+  *out = op;
+  return CFDB_OK;
+}
+
+cfdb_status cfdb_poperator_create_faces(cfdb_context* ctx, const cfdb_grid* grid,
+                                        const double* face_coeff_host, int pinned,
+                                        int64_t reference_cell, cfdb_poperator** out) {
+  if (!ctx || !out || !face_coeff_host) return CFDB_ERR_INVALID_ARGUMENT;
+  CFDB_CUDA(ctx, cudaSetDevice(ctx->device));
+  cfdb_poperator* op = nullptr;
+  cfdb_status st = new_operator(ctx, grid, pinned, reference_cell, &op);
+  if (st != CFDB_OK) return st;
+  st = build_tables(ctx, op, 1.0, 0u);  // zero-filled fallbacks for absent axes
+  if (st != CFDB_OK) {
+    cfdb_poperator_destroy(op);
+    return st;
+  }
+  const cfdb_grid& g = *grid;
+  const int64_t nx = g.n[0], ny = g.n[1], nz = g.dim == 3 ? g.n[2] : 1;
+  const int64_t nfx = (nx + 1) * ny * nz, nfy = nx * (ny + 1) * nz, nfz = g.dim == 3 ? nx * ny * (nz + 1) : 0;
+  const int64_t counts[3] = {nfx, nfy, nfz};
+  const int64_t offs[3] = {0, nfx, nfx + nfy};
+  // real axis -> kernel axis: 2D y-faces become kernel z-faces
+  const int kaxis[3] = {0, g.dim == 2 ? 2 : 1, 2};
+  for (int a = 0; a < g.dim; ++a) {
+    const int ka = kaxis[a];
+    const int64_t m = counts[a];
+    for (int64_t q = 0; q < m; ++q)
+      if (!std::isfinite(face_coeff_host[offs[a] + q])) {
+        cfdb_poperator_destroy(op);
+        return set_error(ctx, CFDB_ERR_INVALID_ARGUMENT, "non-finite face coefficient");
+      }
+    std::vector<float> f32(m);
+    for (int64_t q = 0; q < m; ++q) f32[q] = (float)face_coeff_host[offs[a] + q];
+    cudaError_t e1 = cudaMalloc((void**)&op->f64[ka], m * sizeof(double));
+    cudaError_t e2 = cudaMalloc((void**)&op->f32[ka], m * sizeof(float));
+    if (e1 != cudaSuccess || e2 != cudaSuccess) {
+      cfdb_poperator_destroy(op);
+      return set_error(ctx, CFDB_ERR_OUT_OF_MEMORY, "face coefficient allocation failed");
+    }
+    CFDB_CUDA(ctx, cudaMemcpy(op->f64[ka], face_coeff_host + offs[a], m * sizeof(double),
+                              cudaMemcpyHostToDevice));
+    CFDB_CUDA(ctx, cudaMemcpy(op->f32[ka], f32.data(), m * sizeof(float), cudaMemcpyHostToDevice));
+  }
+  *out = op;
+  return CFDB_OK;
+}
+
+void cfdb_poperator_destroy(cfdb_poperator* op) {
+  if (!op) return;
+  for (int q = 0; q < 3; ++q) {
+    cudaFree(op->t64[q]);
+    cudaFree(op->t32[q]);
+    cudaFree(op->f64[q]);
+    cudaFree(op->f32[q]);
+  }
+  for (int q = 0; q < 6; ++q) cudaFree(op->w64[q]);
+  for (int q = 0; q < 5; ++q) cudaFree(op->w32[q]);
+  cudaFree(op->hist_dev);
+  delete op;
+}
+
+int64_t cfdb_poperator_cells(const cfdb_poperator* op) { return op ? op->cells : 0; }
+
+cfdb_status cfdb_poperator_apply(cfdb_context* ctx, const cfdb_poperator* op, const double* x_dev,
+                                 double* y_dev) {
+  if (!ctx || !op || !x_dev || !y_dev) return CFDB_ERR_INVALID_ARGUMENT;
+  const OpView<double> A = view<double>(op);
+  if (op->grid.dim == 3) {
+    Tiling tl = make_tiling<32, 8>(op->knx, op->kny, op->knz);
+    const int grid = (int)std::max<int64_t>(1, (tl.items + 15) / 16);
+    apply_kernel<8><<<grid, dim3(32, 8), 0, ctx->stream>>>(A, tl, x_dev, y_dev);
+  } else {
+    Tiling tl = make_tiling<256, 1>(op->knx, op->kny, op->knz);
+    const int grid = (int)std::max<int64_t>(1, (tl.items + 15) / 16);
+    apply_kernel<1><<<grid, dim3(256, 1), 0, ctx->stream>>>(A, tl, x_dev, y_dev);
+  }
+  CFDB_CHECK_LAUNCH(ctx);
+  count_launch(ctx);
+  return CFDB_OK;
+}
+
+cfdb_status cfdb_poperator_solve_device(cfdb_context* ctx, const cfdb_poperator* opc,
+                                        const cfdb_linear_settings* s, const double* b_dev,
+                                        double* x_dev, double* history, int64_t history_cap,
+                                        cfdb_linear_result* result) {
+  if (!ctx || !opc || !s || !b_dev || !x_dev || !result) return CFDB_ERR_INVALID_ARGUMENT;
+  auto* op = const_cast<cfdb_poperator*>(opc);
+  std::memset(result, 0, sizeof(*result));
+  if (s->krylov != CFDB_KRYLOV_CG)
+    return set_error(ctx, CFDB_ERR_UNSUPPORTED, "the structured p' solve runs CG");
+  if (s->preconditioner != CFDB_PRECOND_JACOBI)
+    return set_error(ctx, CFDB_ERR_UNSUPPORTED, "the structured p' solve is Jacobi-preconditioned");
+  if (s->max_iterations < 1)
+    return set_error(ctx, CFDB_ERR_INVALID_ARGUMENT, "max_iterations must be >= 1");
+  if (history_cap < 0) history_cap = 0;
+  CFDB_CUDA(ctx, cudaSetDevice(ctx->device));
+  const int64_t launches0 = ctx->launches;
+  // NonFiniteInput (CG.cpp:23-26): the operator was validated at creation.
+  bool ok_b = true, ok_x = true;
+  cfdb_status st = check_finite(ctx, b_dev, op->cells, &ok_b);
+  if (st != CFDB_OK) return st;
+  st = check_finite(ctx, x_dev, op->cells, &ok_x);
+  if (st != CFDB_OK) return st;
+  if (!ok_b || !ok_x) {
+    result->status = CFDB_SOLVER_NONFINITE_INPUT;
+    return CFDB_OK;
+  }
+  CFDB_CUDA(ctx, cudaEventRecord(ctx->ev_start, ctx->stream));
+  if (s->precision == CFDB_PRECISION_FP32_REFINED) {
+    st = solve_refined(ctx, op, s, b_dev, x_dev, history_cap, history, result);
+  } else {
+    st = solve_fp64(ctx, op, s, b_dev, x_dev, false, history_cap, result);
+    if (st == CFDB_OK && history && history_cap > 0) {
+      const int64_t m = std::min<int64_t>(history_cap, result->iterations + 1);
+      CFDB_CUDA(ctx, cudaMemcpyAsync(history, op->hist_dev, sizeof(double) * m,
+                                     cudaMemcpyDeviceToHost, ctx->stream));
+    }
+  }
+  if (st != CFDB_OK) return st;
+  CFDB_CUDA(ctx, cudaEventRecord(ctx->ev_stop, ctx->stream));
+  CFDB_CUDA(ctx, cudaEventSynchronize(ctx->ev_stop));
+  float ms = 0.f;
+  CFDB_CUDA(ctx, cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop));
+  result->device_ms = ms;
+  // FP64 true residual of the returned x (outside the timed region).
+  double tr = 0.0;
+  st = refine_pass(ctx, op, b_dev, x_dev, nullptr, nullptr, 0.0, nullptr, nullptr, &tr);
+  if (st != CFDB_OK) return st;
+  result->true_residual = tr;
+  result->kernel_launches = ctx->launches - launches0;
+  return CFDB_OK;
+}
+
+cfdb_status cfdb_poperator_solve_host(cfdb_context* ctx, const cfdb_poperator* opc,
+                                      const cfdb_linear_settings* s, const double* b_host,
+                                      double* x_host, double* history, int64_t history_cap,
+                                      cfdb_linear_result* result) {
+  if (!ctx || !opc || !b_host || !x_host) return CFDB_ERR_INVALID_ARGUMENT;
+  auto* op = const_cast<cfdb_poperator*>(opc);
+  CFDB_CUDA(ctx, cudaSetDevice(ctx->device));
+  const size_t bytes = sizeof(double) * (size_t)op->cells;
+  for (int q = 4; q < 6; ++q) {
+    cfdb_status st = alloc_vec(ctx, &op->w64[q], op->cells);
+    if (st != CFDB_OK) return st;
+  }
+  CFDB_CUDA(ctx, cudaMemcpyAsync(op->w64[4], b_host, bytes, cudaMemcpyHostToDevice, ctx->stream));
+  CFDB_CUDA(ctx, cudaMemcpyAsync(op->w64[5], x_host, bytes, cudaMemcpyHostToDevice, ctx->stream));
+  cfdb_status st = cfdb_poperator_solve_device(ctx, op, s, op->w64[4], op->w64[5], history,
+                                               history_cap, result);
+  if (st != CFDB_OK) return st;
+  CFDB_CUDA(ctx, cudaMemcpyAsync(x_host, op->w64[5], bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  CFDB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return CFDB_OK;
+}
+
+}  // extern "C"

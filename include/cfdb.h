@@ -1,0 +1,191 @@
+/* cfdb -- C ABI of the B200-native SIMPLE pressure-velocity path.
+ *
+ * Plain C types only (pointers, sizes, PODs): no C++, no torch.  Every entry
+ * point returns a cfdb_status; on error the context keeps a message readable
+ * with cfdb_last_error().  Calls on one context must be serialised by the
+ * caller (the reference's GPU solvers carry the same one-host-thread rule,
+ * GpuLinearSolverCuda.cpp:327-334); distinct contexts are independent.
+ *
+ * Layout of every field (shared with the reference's Cartesian meshes,
+ * MeshGeometry.cpp:417-476 and :1047-1140):
+ *   cell (i,j,k)     -> i + nx*(j + ny*k)                (2D: k = 0)
+ *   faces, global order: x-faces, then y-faces, then z-faces
+ *     x-face (i,j,k), i in [0,nx]: i + (nx+1)*(j + ny*k)
+ *     y-face (i,j,k), j in [0,ny]: i + nx*(j + (ny+1)*k)
+ *     z-face (i,j,k), k in [0,nz]: i + nx*(j + ny*k)
+ *   patches: 0 xmin (left) 1 xmax (right) 2 ymin (bottom) 3 ymax (top) 4 zmin 5 zmax
+ */
+#ifndef CFDB_H
+#define CFDB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define CFDB_API __attribute__((visibility("default")))
+#else
+#define CFDB_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int cfdb_status;
+enum {
+  CFDB_OK = 0,
+  CFDB_ERR_INVALID_ARGUMENT = -1,
+  CFDB_ERR_CUDA = -2,
+  CFDB_ERR_NO_DEVICE = -3,
+  CFDB_ERR_OUT_OF_MEMORY = -4,
+  CFDB_ERR_DEVICE_TIMEOUT = -5, /* a bounded device-side wait gave up (no fault) */
+  CFDB_ERR_UNSUPPORTED = -6
+};
+
+/* Linear-solve outcome, SolverStatus (include/cfd/algebra/LinearSolver.hpp:16-23). */
+enum {
+  CFDB_SOLVER_CONVERGED = 0,
+  CFDB_SOLVER_MAX_ITERATIONS = 1,
+  CFDB_SOLVER_BREAKDOWN = 2,
+  CFDB_SOLVER_NONFINITE_INPUT = 3,
+  CFDB_SOLVER_NONFINITE_RESIDUAL = 4,
+  CFDB_SOLVER_INVALID_SYSTEM = 5
+};
+
+/* SIMPLE outcome, SIMPLEStatus (include/cfd/pressure_velocity/SIMPLEResult.hpp:21-31). */
+enum {
+  CFDB_SIMPLE_CONVERGED = 0,
+  CFDB_SIMPLE_MAX_ITERATIONS = 1,
+  CFDB_SIMPLE_MOMENTUM_FAILURE = 2,
+  CFDB_SIMPLE_PRESSURE_FAILURE = 3,
+  CFDB_SIMPLE_NONFINITE_STATE = 4,
+  CFDB_SIMPLE_INVALID_CONFIGURATION = 5
+};
+
+typedef struct cfdb_context cfdb_context;
+typedef struct cfdb_poperator cfdb_poperator;
+
+typedef struct {
+  int dim;        /* 2 or 3 */
+  int64_t n[3];   /* cells per axis; n[2] ignored in 2D */
+  double len[3];  /* domain lengths; len[2] ignored in 2D */
+} cfdb_grid;
+
+/* Krylov method / precision / preconditioner selection. */
+enum { CFDB_KRYLOV_CG = 0, CFDB_KRYLOV_BICGSTAB = 1 };
+enum {
+  CFDB_PRECISION_FP64 = 0,          /* every sweep in FP64 (the reference's arithmetic) */
+  CFDB_PRECISION_FP32_REFINED = 1   /* FP32 inner sweeps inside FP64 iterative refinement */
+};
+enum { CFDB_PRECOND_NONE = 0, CFDB_PRECOND_JACOBI = 1 };
+
+/* LinearSolverSettings (LinearSolver.hpp:136-166) plus the precision knobs. */
+typedef struct {
+  int krylov;             /* CFDB_KRYLOV_* */
+  int preconditioner;     /* CFDB_PRECOND_* */
+  int precision;          /* CFDB_PRECISION_* */
+  double abs_tol;         /* ||r||_2 <= abs_tol, or */
+  double rel_tol;         /* ||r||_2 / ||r0||_2 <= rel_tol (unpreconditioned residual) */
+  int64_t max_iterations; /* FP64: Krylov iterations; FP32_REFINED: total inner iterations */
+  double inner_rel_tol;   /* FP32_REFINED: reduction asked of each inner solve (0 = default) */
+  int64_t max_refinements;/* FP32_REFINED: outer FP64 refinement steps (0 = default) */
+} cfdb_linear_settings;
+
+/* SolverResult (LinearSolver.hpp:110-134) plus refinement counters. */
+typedef struct {
+  int status;                 /* CFDB_SOLVER_* */
+  int64_t iterations;         /* Krylov iterations (FP32_REFINED: inner iterations, summed) */
+  double initial_residual;    /* ||b - A x0||_2 */
+  double final_residual;      /* ||b - A x||_2 as the method tracks it */
+  double true_residual;       /* FP64-recomputed ||b - A x||_2 of the returned x */
+  int64_t refinements;        /* FP32_REFINED: outer FP64 steps taken */
+  int64_t restarts;           /* BiCGSTAB restarts */
+  double device_ms;           /* device time of the solve (CUDA events, launching stream) */
+  int64_t kernel_launches;    /* kernels this library launched for the solve */
+  double krylov_ms;           /* device time inside the persistent Krylov kernels */
+  double krylov_bytes;        /* algorithmic bytes those kernels move (words read + written) */
+  int64_t krylov_launches;    /* number of persistent Krylov kernel launches */
+} cfdb_linear_result;
+
+/* ------------------------------------------------------------------ context */
+
+/* cudaAvailable() (include/cfd/gpu/GPUBackend.hpp:15): 1 if a CUDA device of
+ * compute capability 10.x is usable, else 0.  Never fails loudly. */
+CFDB_API int cfdb_cuda_available(void);
+
+/* One context per device and host thread.  stream may be NULL (the context
+ * creates its own non-blocking stream) or a caller cudaStream_t. */
+CFDB_API cfdb_status cfdb_create(int device, void* stream, cfdb_context** out);
+CFDB_API void cfdb_destroy(cfdb_context* ctx);
+CFDB_API const char* cfdb_last_error(const cfdb_context* ctx);
+/* The cudaStream_t every call of this context launches on. */
+CFDB_API void* cfdb_stream(cfdb_context* ctx);
+/* Number of kernels this context launched so far (instrumentation). */
+CFDB_API int64_t cfdb_kernel_launches(const cfdb_context* ctx);
+
+/* Seeded synthetic p' RHS of the isolated solve (32 random-phase
+ * sinusoids, wavenumbers 1..64, amplitude |k|^-2, zero mean, cell 0 pinned):
+ * host output of nx*ny[*nz] doubles.  nz = 0 selects 2D. */
+CFDB_API cfdb_status cfdb_synth_rhs(int64_t nx, int64_t ny, int64_t nz, uint64_t seed, double* b_host);
+
+/* ------------------------------------------------- structured p' operator */
+
+/* The p' operator of assembleGeometricPressureCorrection
+ * (src/pressure_velocity/PressureCorrectionEquation.cpp:181-339) on a uniform
+ * Cartesian grid, held on the device matrix-free:
+ *   (A x)_P = (sum_f D_f) x_P - sum_{internal f} D_f x_N,
+ * the diagonal summed in face order; when `pinned`, row `reference_cell` is
+ * the identity (the reference pins it when no FixedValue pressure patch
+ * exists, :221-228 and :326-329) while the neighbouring rows keep their
+ * coupling to it.
+ *
+ * _uniform: unit response coefficients and density rho on all faces,
+ *   D_f = rho |S_f| / |d_f| computed from the grid exactly as the reference
+ *   does; boundary faces Neumann (0) unless dirichlet_patch_mask has the
+ *   patch's bit set (then D_b = rho |S_f| / |x_f - x_P|).  This is the
+ *   isolated p' system of the benchmark.
+ * _faces: arbitrary face coefficients (host, global face order, boundary
+ *   faces included: 0 for Neumann), e.g. the faceCoefficient field of a
+ *   SIMPLE iteration. */
+CFDB_API cfdb_status cfdb_poperator_create_uniform(cfdb_context* ctx, const cfdb_grid* grid, double rho,
+                                          unsigned dirichlet_patch_mask, int pinned,
+                                          int64_t reference_cell, cfdb_poperator** out);
+CFDB_API cfdb_status cfdb_poperator_create_faces(cfdb_context* ctx, const cfdb_grid* grid,
+                                        const double* face_coeff_host, int pinned,
+                                        int64_t reference_cell, cfdb_poperator** out);
+CFDB_API void cfdb_poperator_destroy(cfdb_poperator* op);
+CFDB_API int64_t cfdb_poperator_cells(const cfdb_poperator* op);
+
+/* y = A x on device pointers (FP64). */
+CFDB_API cfdb_status cfdb_poperator_apply(cfdb_context* ctx, const cfdb_poperator* op, const double* x_dev,
+                                 double* y_dev);
+
+/* Solve A x = b.  Replaces the reference's CG::solve / BiCGSTAB::solve
+ * (src/algebra/CG.cpp:14-148) for this operator, same status semantics and
+ * convergence test.
+ *   _device: b_dev, x_dev (x0 on entry, solution on exit) are device pointers;
+ *   _host:   host pointers, copied in and out inside the call.
+ * history (host, may be NULL) receives residualHistory: entry 0 = ||r0||,
+ * entry k = ||r|| after iteration k, at most history_cap entries. */
+CFDB_API cfdb_status cfdb_poperator_solve_device(cfdb_context* ctx, const cfdb_poperator* op,
+                                        const cfdb_linear_settings* settings, const double* b_dev,
+                                        double* x_dev, double* history, int64_t history_cap,
+                                        cfdb_linear_result* result);
+CFDB_API cfdb_status cfdb_poperator_solve_host(cfdb_context* ctx, const cfdb_poperator* op,
+                                      const cfdb_linear_settings* settings, const double* b_host,
+                                      double* x_host, double* history, int64_t history_cap,
+                                      cfdb_linear_result* result);
+
+/* Device buffers owned by the context's allocator (for callers without a
+ * CUDA runtime of their own: tests, FFI hosts). */
+CFDB_API cfdb_status cfdb_device_alloc(cfdb_context* ctx, size_t bytes, void** out);
+CFDB_API cfdb_status cfdb_device_free(cfdb_context* ctx, void* ptr);
+CFDB_API cfdb_status cfdb_copy_to_device(cfdb_context* ctx, void* dst_dev, const void* src_host, size_t bytes);
+CFDB_API cfdb_status cfdb_copy_to_host(cfdb_context* ctx, void* dst_host, const void* src_dev, size_t bytes);
+CFDB_API cfdb_status cfdb_memset_device(cfdb_context* ctx, void* dst_dev, int value, size_t bytes);
+CFDB_API cfdb_status cfdb_synchronize(cfdb_context* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -6,7 +6,8 @@
 // Commands (key=value arguments, binary float64 outputs under out=DIR):
 //
 //   poisson dim=2|3 n=N [seed=S] [rtol=1e-8] [maxit=M] [pre=jacobi|none]
-//           [solver=cg|bicgstab] [out=DIR] [dump_matrix=1]
+//           [solver=cg|bicgstab] [out=DIR] [dump_matrix=1] [direct=1] [repeat=R]
+//           [check_direct=1]
 //       p' system of the reference's assemblePressureCorrection
 //       (PressureCorrectionEquation.cpp:341) with unit response
 //       coefficients, rho = 1, all-FixedGradient(0) pressure patches and
@@ -27,6 +28,7 @@
 //       {inlet,0} left, Outlet right, Walls; pressure FixedValue(0) at the
 //       outlet), pressure FixedGradient(0) elsewhere.  Writes u v [w] p flux
 //       and the residual histories.
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -55,6 +57,13 @@
 #include "cfd/pressure_velocity/PressureCorrectionEquation.hpp"
 #include "cfd/pressure_velocity/SIMPLE.hpp"
 #include "synth_rhs.h"
+
+#ifdef _OPENMP
+#include <omp.h>
+static int ompThreads() { return omp_get_max_threads(); }
+#else
+static int ompThreads() { return 1; }
+#endif
 
 using namespace cfd;
 
@@ -117,14 +126,11 @@ mesh::Mesh makeMesh(int dim, long long nx, long long ny, long long nz, double lx
   return mesh::MeshGeometry::createCartesian2D(nx, ny, lx, ly);
 }
 
-int runPoisson(const Args& a) {
-  const int dim = static_cast<int>(geti(a, "dim", 2));
-  const long long n = geti(a, "n", 64);
-  const auto seed = static_cast<uint64_t>(geti(a, "seed", 20261203));
-  const std::string out = get(a, "out", "");
-  const mesh::Mesh m = makeMesh(dim, n, n, n, 1.0, 1.0, 1.0);
+// The isolated p' matrix through the reference's own assembly
+// (assemblePressureCorrection with unit response, rho = 1, Neumann patches,
+// cell 0 pinned).
+algebra::SparseMatrix referenceMatrix(const mesh::Mesh& m, int dim) {
   const Index cells = m.numberOfCells();
-
   boundary::BoundaryConditionSet pBCs;
   for (const auto& patch : m.boundaryPatches())
     pBCs.set(m, patch.name(), std::make_unique<boundary::FixedGradient>(0.0));
@@ -133,12 +139,79 @@ int runPoisson(const Args& a) {
   pressure_velocity::PressureCorrectionOptions opts;
   auto assembly = pressure_velocity::assemblePressureCorrection(
       m, zeroFlux, one, one, 1.0, 0, pBCs, opts, dim == 3 ? &one : nullptr);
+  return algebra::SparseMatrix(assembly.system.matrix());
+}
+
+// The same matrix written directly in CSR (ascending columns, diagonal summed
+// in face order, same coefficient expression), O(n) instead of the triplet
+// sort: only used to keep the timed CPU-baseline setup short at 2048^2 /
+// 256^3; `check_direct=1` verifies it equals referenceMatrix bit for bit.
+algebra::SparseMatrix directMatrix(const mesh::Mesh& m, int dim, long long n) {
+  const Index cells = m.numberOfCells();
+  const double delta = 1.0 / static_cast<double>(n);
+  const double area = dim == 3 ? delta * delta : delta;
+  std::vector<double> coef(n + 1, 0.0);
+  for (long long f = 1; f < n; ++f) {
+    const double cP = (static_cast<double>(f - 1) + 0.5) * delta;
+    const double cN = (static_cast<double>(f) + 0.5) * delta;
+    const double node = static_cast<double>(f) * delta;
+    const double dPf = std::fabs(node - cP), dNf = std::fabs(node - cN);
+    const double dFace = ((dNf * 1.0) + (dPf * 1.0)) / (dPf + dNf);
+    coef[f] = 1.0 * area * dFace / std::fabs(cN - cP);
+  }
+  const long long nx = n, ny = n, nz = dim == 3 ? n : 1;
+  const long long stride[3] = {1, nx, nx * ny};
+  std::vector<Index> offsets(cells + 1, 0);
+  std::vector<Index> cols;
+  std::vector<double> vals;
+  cols.reserve(cells * (dim == 3 ? 7 : 5));
+  vals.reserve(cells * (dim == 3 ? 7 : 5));
+  for (Index c = 0; c < cells; ++c) {
+    const long long ijk[3] = {static_cast<long long>(c % nx), static_cast<long long>((c / nx) % ny),
+                              static_cast<long long>(c / (nx * ny))};
+    if (c == 0) {
+      cols.push_back(0);
+      vals.push_back(1.0);
+      offsets[c + 1] = cols.size();
+      continue;
+    }
+    double diag = 0.0;
+    for (int ax = 0; ax < dim; ++ax) {
+      if (ijk[ax] > 0) diag += coef[ijk[ax]];
+      if (ijk[ax] < (ax == 2 ? nz : (ax == 1 ? ny : nx)) - 1) diag += coef[ijk[ax] + 1];
+    }
+    for (int ax = dim - 1; ax >= 0; --ax)
+      if (ijk[ax] > 0) {
+        cols.push_back(c - stride[ax]);
+        vals.push_back(-coef[ijk[ax]]);
+      }
+    cols.push_back(c);
+    vals.push_back(diag);
+    for (int ax = 0; ax < dim; ++ax)
+      if (ijk[ax] < (ax == 2 ? nz : (ax == 1 ? ny : nx)) - 1) {
+        cols.push_back(c + stride[ax]);
+        vals.push_back(-coef[ijk[ax] + 1]);
+      }
+    offsets[c + 1] = cols.size();
+  }
+  return algebra::SparseMatrix(cells, cells, std::move(vals), std::move(cols), std::move(offsets));
+}
+
+int runPoisson(const Args& a) {
+  const int dim = static_cast<int>(geti(a, "dim", 2));
+  const long long n = geti(a, "n", 64);
+  const auto seed = static_cast<uint64_t>(geti(a, "seed", 20261203));
+  const std::string out = get(a, "out", "");
+  const mesh::Mesh m = makeMesh(dim, n, n, n, 1.0, 1.0, 1.0);
+  const Index cells = m.numberOfCells();
 
   std::vector<double> b(cells);
   oracle_synth_rhs(n, n, dim == 3 ? n : 0, seed, b.data());
   algebra::Vector rhs(cells);
   for (Index i = 0; i < cells; ++i) rhs[i] = b[i];
-  const algebra::LinearSystem system(algebra::SparseMatrix(assembly.system.matrix()), rhs);
+  const bool direct = geti(a, "direct", 0) != 0;
+  const algebra::LinearSystem system(direct ? directMatrix(m, dim, n) : referenceMatrix(m, dim),
+                                     rhs);
 
   algebra::LinearSolverSettings s;
   s.absoluteTolerance = getd(a, "atol", 0.0);
@@ -152,10 +225,27 @@ int runPoisson(const Args& a) {
   else
     solver = std::make_unique<algebra::CG>(s, pre);
 
-  const auto t0 = std::chrono::steady_clock::now();
-  const algebra::SolverResult r = solver->solve(system);
-  const auto t1 = std::chrono::steady_clock::now();
-  const double seconds = std::chrono::duration<double>(t1 - t0).count();
+  if (geti(a, "check_direct", 0) != 0) {
+    const algebra::SparseMatrix A = referenceMatrix(m, dim), B = directMatrix(m, dim, n);
+    bool same = A.nonZeros() == B.nonZeros();
+    for (Index k = 0; same && k < A.nonZeros(); ++k)
+      same = A.valuesData()[k] == B.valuesData()[k] && A.columnIndicesData()[k] == B.columnIndicesData()[k];
+    for (Index r = 0; same && r <= A.rows(); ++r) same = A.rowOffsetsData()[r] == B.rowOffsetsData()[r];
+    std::printf("{\"direct_matches_reference\": %s}\n", same ? "true" : "false");
+    return same ? 0 : 1;
+  }
+  // repeat=R times the same solve R times (each from x0 = 0); the summary
+  // reports the last one and `repeat_seconds` lists all.
+  const long long repeat = std::max(1LL, geti(a, "repeat", 1));
+  std::string times;
+  algebra::SolverResult r;
+  double seconds = 0.0;
+  for (long long q = 0; q < repeat; ++q) {
+    const auto t0 = std::chrono::steady_clock::now();
+    r = solver->solve(system);
+    seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    times += (q ? ", " : "") + std::to_string(seconds);
+  }
 
   // FP64 true residual of the returned solution.
   const algebra::Vector ax = system.matrix().multiply(r.solution);
@@ -168,10 +258,10 @@ int runPoisson(const Args& a) {
   std::printf(
       "{\"status\": \"%s\", \"iterations\": %zu, \"initial_residual\": %.17g, "
       "\"final_residual\": %.17g, \"true_rel_residual\": %.17g, \"seconds\": %.6f, "
-      "\"cells\": %zu, \"nnz\": %zu}\n",
+      "\"cells\": %zu, \"nnz\": %zu, \"threads\": %d, \"repeat_seconds\": [%s]}\n",
       solverStatusText(r.status), static_cast<size_t>(r.iterations), r.initialResidual,
       r.finalResidual, std::sqrt(rr) / std::sqrt(bb), seconds, static_cast<size_t>(cells),
-      static_cast<size_t>(system.matrix().nonZeros()));
+      static_cast<size_t>(system.matrix().nonZeros()), ompThreads(), times.c_str());
   if (!out.empty()) {
     writeBin(out + "/rhs.bin", b);
     writeBin(out + "/x.bin", r.solution.data(), cells);

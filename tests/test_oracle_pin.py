@@ -1,0 +1,109 @@
+"""Pins the CPU oracle (oracle/cfdb_oracle.c) to the reference.
+
+Two sources: the committed fixtures under tests/golden/ (generated by the
+reference's own code, tests/golden/make_golden.py) and, when it is built here,
+the reference itself (oracle/_ref/ref_driver).  The bar is bit-identity: the
+oracle restates the reference's arithmetic in the same order.
+"""
+import json
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def _kv(args):
+    return dict(a.split("=", 1) for a in args.split())
+
+
+def simple_from_args(args):
+    """Oracle case + settings equivalent to a ref_driver `simple` argument string."""
+    a = _kv(args)
+    dim = int(a.get("dim", 2))
+    nx = int(a["nx"])
+    ny = int(a.get("ny", nx))
+    nz = int(a.get("nz", nx))
+    if a.get("flow", "cavity") == "channel":
+        case = O.channel(nx, ny, float(a.get("lx", 1)), float(a.get("ly", 1)),
+                         float(a.get("inlet", 1)))
+    else:
+        case = O.cavity(dim, nx, float(a.get("lid", 1)))
+        case.n = (nx, ny, nz)[:dim]
+    s = O.SimpleSettings(
+        max_outer=int(a.get("outer", 1000)), alpha_u=float(a.get("au", 0.7)),
+        alpha_p=float(a.get("ap", 0.3)), tol_u=float(a.get("tolu", 1e-6)),
+        tol_p=float(a.get("tolp", 1e-6)), tol_c=float(a.get("tolc", 1e-6)),
+        rho=float(a.get("rho", 1)), mu=float(a.get("mu", 0.01)),
+        scheme=a.get("scheme", "upwind"), face_flux=a.get("flux", "auto"),
+        momentum=(a.get("msolver", "bicgstab"), a.get("mpre", "none") == "jacobi",
+                  float(a.get("mabs", 1e-10)), float(a.get("mrel", 1e-8)), int(a.get("mmax", 500))),
+        pressure=(a.get("psolver", "cg"), a.get("ppre", "jacobi") == "jacobi",
+                  float(a.get("pabs", 0.0)), float(a.get("prel", 1e-8)), int(a.get("pmax", 5000))))
+    return case, s
+
+
+def _fixtures(prefix):
+    return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.startswith(prefix) and f.endswith(".npz"))
+
+
+@pytest.mark.parametrize("name", _fixtures("poisson"))
+def test_poisson_matches_golden(name):
+    g = np.load(os.path.join(GOLDEN, name + ".npz"))
+    meta = json.loads(str(g["meta"]))
+    a = _kv(meta["args"])
+    case, fc, diag, off, b = O.isolated_pprime(int(a["dim"]), int(a["n"]))
+    assert np.array_equal(b, g["rhs"]), "synthetic RHS differs from the reference driver's"
+    r = O.stencil_solve(case, diag, off, b)
+    assert r.status == meta["status"]
+    assert r.iterations == meta["iterations"]
+    assert np.array_equal(r.history, g["hist"])
+    assert np.array_equal(r.solution, g["x"])
+
+
+@pytest.mark.parametrize("name", [n for n in _fixtures("")
+                                  if not n.startswith("poisson")])
+def test_simple_matches_golden(name):
+    g = np.load(os.path.join(GOLDEN, name + ".npz"))
+    meta = json.loads(str(g["meta"]))
+    case, s = simple_from_args(meta["args"])
+    r = O.simple(case, s)
+    assert r.status == meta["status"]
+    assert r.iterations == meta["iterations"]
+    for f in ("u", "v", "w", "p", "flux"):
+        if f in g.files:
+            assert np.array_equal(getattr(r, f), g[f]), f
+    hist = g["hist"].reshape(-1, 5)
+    assert np.array_equal(r.history, hist)
+
+
+def test_synth_rhs_zero_mean_and_pin():
+    b = O.synth_rhs(2, 32)
+    assert b[0] == 0.0
+    # zero mean before the pin: what is left is (minus) the pinned entry
+    assert abs(b.sum()) <= 2.0 * np.abs(b).max()
+
+
+@pytest.mark.skipif(not O.ref_driver_available(), reason="reference not built (oracle/_ref)")
+@pytest.mark.parametrize("args", [
+    "dim=2 nx=12 ny=10 outer=60 scheme=quick flux=rhiechow",
+    "dim=2 nx=24 ny=6 lx=4 ly=1 flow=channel mu=0.05 scheme=lud outer=40",
+    "dim=3 nx=6 ny=5 nz=4 outer=15 scheme=lud",
+])
+def test_oracle_matches_reference_build(args):
+    """Live pin against the reference compiled from its own sources."""
+    with tempfile.TemporaryDirectory() as d:
+        out = subprocess.run([O.REF_DRIVER, "simple"] + args.split() + [f"out={d}"],
+                             capture_output=True, text=True, check=True,
+                             env=dict(os.environ, OMP_NUM_THREADS="1"))
+        meta = json.loads(out.stdout)
+        case, s = simple_from_args(args)
+        r = O.simple(case, s)
+        assert r.status == meta["status"] and r.iterations == meta["iterations"]
+        for f in ("u", "v", "p", "flux") + (("w",) if case.dim == 3 else ()):
+            assert np.array_equal(getattr(r, f), np.fromfile(os.path.join(d, f + ".bin"))), f

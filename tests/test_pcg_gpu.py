@@ -1,0 +1,119 @@
+"""Parity of the device p' solves with the CPU oracle (which is bit-identical
+to the reference's CG + Jacobi, tests/test_oracle_pin.py).
+
+Bars: same status; iteration count within +-2 % of the oracle's (the device
+sums its dot products in a different order); residual histories within 1e-6
+relative; solutions within 1e-9 relative L2 (FP64) and 1e-7 (FP32-refined,
+which must still reach the FP64-verified 1e-8 relative residual).
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _settings(**kw):
+    from cfdapp_b200.cfdb import LinearSolverSettings
+    base = dict(absolute_tolerance=0.0, relative_tolerance=1e-8, max_iterations=100000)
+    base.update(kw)
+    return LinearSolverSettings(**base)
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+@pytest.mark.parametrize("dim,n", [(2, 64), (2, 200), (3, 16), (3, 40), (2, 513)])
+def test_isolated_fp64_matches_oracle(ctx, dim, n):
+    from cfdapp_b200.cfdb import POperator
+    case, fc, diag, off, b = O.isolated_pprime(dim, n)
+    ref = O.stencil_solve(case, diag, off, b)
+    op = POperator(ctx, dim, [n] * dim)
+    res = op.solve(b, _settings())
+    assert res.status == ref.status == "Converged"
+    assert abs(res.iterations - ref.iterations) <= max(2, 0.02 * ref.iterations)
+    m = min(len(res.residual_history), len(ref.history))
+    np.testing.assert_allclose(res.residual_history[:m], ref.history[:m], rtol=1e-6)
+    assert _rel(res.solution, ref.solution) <= 1e-9
+    assert res.true_residual / res.initial_residual <= 1e-8 * 1.01
+    assert res.kernel_launches >= 1
+
+
+@pytest.mark.parametrize("dim,n", [(2, 64), (2, 300), (3, 24)])
+def test_isolated_fp32_refined_reaches_fp64_tolerance(ctx, dim, n):
+    from cfdapp_b200.cfdb import POperator
+    case, fc, diag, off, b = O.isolated_pprime(dim, n)
+    ref = O.stencil_solve(case, diag, off, b)
+    op = POperator(ctx, dim, [n] * dim)
+    res = op.solve(b, _settings(precision="fp32_refined"))
+    assert res.status == "Converged"
+    assert res.true_residual / res.initial_residual <= 1e-8
+    assert res.refinements >= 1
+    # true residual recomputed on the CPU from the returned x
+    ax = O.stencil_apply(case, diag, off, res.solution)
+    assert np.linalg.norm(b - ax) / np.linalg.norm(b) <= 1.01e-8
+    assert _rel(res.solution, ref.solution) <= 1e-6
+
+
+@pytest.mark.parametrize("dim,n", [(2, 40), (3, 12)])
+def test_face_coefficients_match_oracle(ctx, dim, n):
+    """Variable face coefficients (a SIMPLE-like p' system) in face mode."""
+    from cfdapp_b200.cfdb import POperator
+    rng = np.random.default_rng(7)
+    case = O.cavity(dim, n)
+    cells = case.cells()
+    du, dv, dw = (rng.uniform(0.5, 2.0, cells) for _ in range(3))
+    flux = rng.normal(size=case.faces()) * 1e-3
+    fc, diag, off, rhs = O.assemble_pprime(case, 1.0, flux, du, dv, dw)
+    ref = O.stencil_solve(case, diag, off, rhs)
+    op = POperator(ctx, dim, [n] * dim, face_coeff=fc)
+    ax_gpu = op.apply(ref.solution)
+    ax_cpu = O.stencil_apply(case, diag, off, ref.solution)
+    np.testing.assert_allclose(ax_gpu, ax_cpu, rtol=1e-12, atol=1e-14 * np.abs(ax_cpu).max())
+    res = op.solve(rhs, _settings())
+    assert res.status == ref.status == "Converged"
+    assert abs(res.iterations - ref.iterations) <= max(2, 0.02 * ref.iterations)
+    assert _rel(res.solution, ref.solution) <= 1e-9
+
+
+def test_dirichlet_patch_unpinned(ctx):
+    """A FixedValue (Dirichlet) pressure patch: no pin, boundary coefficient on the diagonal."""
+    from cfdapp_b200.cfdb import POperator
+    case = O.channel(48, 12, 4.0, 1.0)
+    cells = case.cells()
+    ones = np.ones(cells)
+    rng = np.random.default_rng(3)
+    flux = rng.normal(size=case.faces()) * 1e-2
+    fc, diag, off, rhs = O.assemble_pprime(case, 1.0, flux, ones, ones)
+    ref = O.stencil_solve(case, diag, off, rhs)
+    op = POperator(ctx, 2, (48, 12), (4.0, 1.0), face_coeff=fc, pinned=False)
+    res = op.solve(rhs, _settings())
+    assert res.status == ref.status == "Converged"
+    assert _rel(res.solution, ref.solution) <= 1e-9
+    op2 = POperator(ctx, 2, (48, 12), (4.0, 1.0), dirichlet_patch_mask=1 << 1, pinned=False)
+    fc2, diag2, off2, _ = O.assemble_pprime(case, 1.0, flux, ones, ones)
+    x = rng.normal(size=cells)
+    np.testing.assert_allclose(op2.apply(x), O.stencil_apply(case, diag2, off2, x), rtol=1e-12,
+                               atol=1e-12)
+
+
+def test_status_edge_cases(ctx):
+    from cfdapp_b200.cfdb import POperator
+    op = POperator(ctx, 2, (32, 32))
+    zero = op.solve(np.zeros(1024), _settings())
+    assert zero.status == "Converged" and zero.iterations == 0
+    b = O.synth_rhs(2, 32)
+    capped = op.solve(b, _settings(max_iterations=5))
+    assert capped.status == "MaxIterations" and capped.iterations == 5
+    bad = b.copy()
+    bad[17] = np.nan
+    assert op.solve(bad, _settings()).status == "NonFiniteInput"
+    # absolute tolerance met by the initial residual
+    loose = op.solve(b, _settings(absolute_tolerance=1.0))
+    assert loose.status == "Converged" and loose.iterations == 0
+    # a warm start at the solution converges immediately
+    sol = op.solve(b, _settings()).solution
+    again = op.solve(b, _settings(relative_tolerance=1e-6), x0=sol)
+    assert again.status == "Converged" and again.iterations <= 1
