@@ -40,6 +40,9 @@ __device__ __forceinline__ bool grid_sync(const GridSync& s) {
     volatile unsigned* vgen = s.gen;
     volatile unsigned* verr = s.error;
     const unsigned g = *vgen;
+    // Global data this block wrote with ordinary stores may be read after the
+    // barrier by TMA (the async proxy) in other blocks: proxy fence first.
+    asm volatile("fence.proxy.async.global;" ::: "memory");
     __threadfence();
     const unsigned prev = atomicAdd(s.count, 1u);
     int good = (*verr == 0u);
@@ -63,6 +66,7 @@ __device__ __forceinline__ bool grid_sync(const GridSync& s) {
       }
     }
     __threadfence();
+    asm volatile("fence.proxy.async.global;" ::: "memory");
     ok_shared = good;
   }
   __syncthreads();

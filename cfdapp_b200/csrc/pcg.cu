@@ -21,6 +21,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -28,6 +29,8 @@
 #include "cfdb_internal.cuh"
 #include "grid_sync.cuh"
 #include "poperator.cuh"
+#include "tile.cuh"
+#include "tma.cuh"
 
 struct cfdb_poperator {
   cfdb_context* ctx = nullptr;
@@ -46,6 +49,8 @@ struct cfdb_poperator {
   float* w32[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};   // r p0 p1 e b32
   double* hist_dev = nullptr;
   int64_t hist_cap = 0;
+  double* invd64 = nullptr;  // 1/diag, face-coefficient operators only
+  float* invd32 = nullptr;
 };
 
 namespace cfdb {
@@ -77,7 +82,8 @@ OpView<T> view(const cfdb_poperator* op) {
 template <typename T>
 struct PcgParams {
   OpView<T> A;
-  Tiling tl;
+  ColumnSplit cs;
+  const T* invd;  // precomputed 1/diag (face-coefficient operators) or null
   const T* b;
   T* x;
   T* r;
@@ -95,14 +101,21 @@ struct PcgParams {
 
 __device__ __forceinline__ bool finite(double v) { return isfinite(v); }
 
-template <typename T, int PY>
-__global__ void __launch_bounds__(kThreads, 3) pcg_persistent(PcgParams<T> P) {
-  constexpr int PX = kThreads / PY;
-  __shared__ T buf[2][PY + 2][PX + 2];
+template <typename T>
+__device__ __forceinline__ T inv_at(const OpView<T>& A, const T* invd, int i, int j, int k) {
+  if (invd) return __ldg(invd + (i + (int64_t)A.nx * (j + (int64_t)A.ny * k)));
+  return load_coef(A, i, j, k).inv;
+}
+
+template <typename T, class S>
+__global__ void __launch_bounds__(kThreads, 2) pcg_persistent(PcgParams<T> P) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* box = reinterpret_cast<T*>(smem_raw);
   __shared__ double red[64];
   const OpView<T>& A = P.A;
   const int B = gridDim.x, blk = blockIdx.x;
   const bool leader = (blockIdx.x == 0 && threadIdx.x == 0 && threadIdx.y == 0);
+  const ColumnSplit cs = P.cs;
   // Partials are double-buffered by reduction round: a block that already
   // summed round k and raced ahead writes round k+1 into the other half while
   // slower blocks may still be reading round k.
@@ -111,26 +124,23 @@ __global__ void __launch_bounds__(kThreads, 3) pcg_persistent(PcgParams<T> P) {
 
   // ---- r0 = b - A x0, ||r0||^2, r0.z0
   double acc[2] = {0.0, 0.0};
-  for_segments(P.tl, A.nz, blk, B, [&](int64_t tile, int k0, int k1) {
-    march<T, PX, PY>(
-        A, P.tl, tile, k0, k1, buf,
-        [&](int i, int j, int k) {
-          const int64_t idx = i + (int64_t)A.nx * (j + (int64_t)A.ny * k);
-          return P.x0_zero ? T(0) : P.x[idx];
-        },
-        [&](int i, int j, int k) {
-          const int64_t idx = i + (int64_t)A.nx * (j + (int64_t)A.ny * k);
-          return P.x0_zero ? T(0) : P.x[idx];
-        },
-        [&](int i, int j, int k, int64_t idx, T v, T w, T e, T s, T n, T bb, T t) {
-          const Coef<T> c = load_coef(A, i, j, k);
-          T rn = __ldg(P.b + idx);
-          if (!P.x0_zero) rn = rn - apply_coef(c, v, w, e, s, n, bb, t);
-          P.r[idx] = rn;
-          const double rd = (double)rn;
-          acc[0] += rd * rd;
-          acc[1] += rd * (double)(c.inv * rn);
-        });
+  for_chunks<S>(cs, A.nz, blk, B, [&](const Chunk& c) {
+    if (!P.x0_zero) {
+      stage_box<S, 8>(A, c, box, [&](int, int, int, int64_t idx) { return P.x[idx]; },
+                      [&](T v, int, int, int) { return v; });
+      __syncthreads();
+    }
+    for_interior<S, 8>(A, c, [&](int64_t idx) { return __ldg(P.b + idx); },
+                       [&](int i, int j, int k, int64_t idx, int e, T bv) {
+      const Coef<T> cf = load_coef(A, i, j, k);
+      T rn = bv;
+      if (!P.x0_zero) rn = rn - apply_box<S>(cf, box, e);
+      P.r[idx] = rn;
+      const double rd = (double)rn;
+      acc[0] += rd * rd;
+      acc[1] += rd * (double)(cf.inv * rn);
+    });
+    __syncthreads();
   });
   block_sum<2>(acc, red);
   if (threadIdx.x == 0 && threadIdx.y == 0) {
@@ -174,24 +184,31 @@ __global__ void __launch_bounds__(kThreads, 3) pcg_persistent(PcgParams<T> P) {
   for (int64_t it = 1; it <= P.max_it; ++it) {
     const bool first = (it == 1);
     const T tbeta = (T)beta;
-    // ---- sweep A: p = z + beta p_old; Ap; p.Ap
+    // ---- sweep A: stage p = D^-1 r + beta p_old over chunk + halo; Ap; p.Ap
     double pap = 0.0;
-    auto pz = [&](int i, int j, int k) {
-      const Coef<T> c = load_coef(A, i, j, k);
-      const int64_t idx = i + (int64_t)A.nx * (j + (int64_t)A.ny * k);
-      const T z = c.inv * __ldcg(P.r + idx);
-      return first ? z : fma(tbeta, __ldcg(pold + idx), z);
-    };
-    for_segments(P.tl, A.nz, blk, B, [&](int64_t tile, int k0, int k1) {
-      march<T, PX, PY>(
-          A, P.tl, tile, k0, k1, buf,
-          pz, pz,
-          [&](int i, int j, int k, int64_t idx, T v, T w, T e, T s, T n, T bb, T t) {
-            const Coef<T> c = load_coef(A, i, j, k);
-            const T ap = apply_coef(c, v, w, e, s, n, bb, t);
-            pnew[idx] = v;
-            pap += (double)v * (double)ap;
+    for_chunks<S>(cs, A.nz, blk, B, [&](const Chunk& c) {
+      stage_box<S, 6>(
+          A, c, box,
+          [&](int, int, int, int64_t idx) {
+            Pair<T> v;
+            v.a = __ldcg(P.r + idx);
+            v.b = first ? T(0) : __ldcg(pold + idx);
+            return v;
+          },
+          [&](Pair<T> v, int i, int j, int k) {
+            const T z = inv_at(A, P.invd, i, j, k) * v.a;
+            return first ? z : fma(tbeta, v.b, z);
           });
+      __syncthreads();
+      for_interior<S, 1>(A, c, [&](int64_t) { return 0; },
+                         [&](int i, int j, int k, int64_t idx, int e, int) {
+        const Coef<T> cf = load_coef(A, i, j, k);
+        const T v = box[e];
+        const T ap = apply_box<S>(cf, box, e);
+        pnew[idx] = v;
+        pap += (double)v * (double)ap;
+      });
+      __syncthreads();
     });
     {
       double a1[1] = {pap};
@@ -215,25 +232,29 @@ __global__ void __launch_bounds__(kThreads, 3) pcg_persistent(PcgParams<T> P) {
     const T talpha = (T)alpha;
     // ---- sweep B: x += alpha p; r -= alpha A p; r.r, r.z
     double ab[2] = {0.0, 0.0};
-    for_segments(P.tl, A.nz, blk, B, [&](int64_t tile, int k0, int k1) {
-      march<T, PX, PY>(
-          A, P.tl, tile, k0, k1, buf,
-          [&](int i, int j, int k) {
-            return __ldcg(pnew + (i + (int64_t)A.nx * (j + (int64_t)A.ny * k)));
+    for_chunks<S>(cs, A.nz, blk, B, [&](const Chunk& c) {
+      stage_box<S, 8>(A, c, box, [&](int, int, int, int64_t idx) { return __ldcg(pnew + idx); },
+                      [&](T v, int, int, int) { return v; });
+      __syncthreads();
+      for_interior<S, 6>(
+          A, c,
+          [&](int64_t idx) {
+            Pair<T> v;
+            v.a = P.x[idx];
+            v.b = P.r[idx];
+            return v;
           },
-          [&](int i, int j, int k) {
-            return __ldcg(pnew + (i + (int64_t)A.nx * (j + (int64_t)A.ny * k)));
-          },
-          [&](int i, int j, int k, int64_t idx, T v, T w, T e, T s, T n, T bb, T t) {
-            const Coef<T> c = load_coef(A, i, j, k);
-            const T ap = apply_coef(c, v, w, e, s, n, bb, t);
-            P.x[idx] = fma(talpha, v, P.x[idx]);
-            const T rn = fma(-talpha, ap, __ldcg(P.r + idx));
-            P.r[idx] = rn;
-            const double rd = (double)rn;
-            ab[0] += rd * rd;
-            ab[1] += rd * (double)(c.inv * rn);
-          });
+          [&](int i, int j, int k, int64_t idx, int e, Pair<T> xr) {
+        const Coef<T> cf = load_coef(A, i, j, k);
+        const T ap = apply_box<S>(cf, box, e);
+        P.x[idx] = fma(talpha, box[e], xr.a);
+        const T rn = fma(-talpha, ap, xr.b);
+        P.r[idx] = rn;
+        const double rd = (double)rn;
+        ab[0] += rd * rd;
+        ab[1] += rd * (double)(cf.inv * rn);
+      });
+      __syncthreads();
     });
     block_sum<2>(ab, red);
     if (threadIdx.x == 0 && threadIdx.y == 0) {
@@ -276,7 +297,6 @@ __global__ void __launch_bounds__(kThreads, 3) pcg_persistent(PcgParams<T> P) {
     T* tmp = pold;
     pold = pnew;
     pnew = tmp;
-    if (leader) P.out[OUT_ITER] = (double)it;
   }
   if (leader) {
     P.out[OUT_STATUS] = CFDB_SOLVER_MAX_ITERATIONS;
@@ -284,6 +304,21 @@ __global__ void __launch_bounds__(kThreads, 3) pcg_persistent(PcgParams<T> P) {
     P.out[OUT_FINAL] = res_cur;
   }
 }
+
+// Inverse diagonal of a face-coefficient operator (computed once per operator).
+template <typename T>
+__global__ void inverse_diagonal(OpView<T> A, T* invd) {
+  const int64_t n = (int64_t)A.nx * A.ny * A.nz;
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(q % A.nx);
+    const int j = (int)((q / A.nx) % A.ny);
+    const int k = (int)(q / ((int64_t)A.nx * A.ny));
+    invd[q] = load_coef(A, i, j, k).inv;
+  }
+}
+
+#include "pcg_tma.cuh"
 
 // FP64 residual pass of the refinement: x_out = x_in + scale * e (e may be
 // null), r = b - A x_out; optionally r32 = (float) r; per-block ||r||^2.
@@ -361,15 +396,17 @@ __global__ void all_finite(const double* v, int64_t n, unsigned* flag) {
 
 bool is3d(const cfdb_poperator* op) { return op->grid.dim == 3; }
 
-template <typename T, int PY>
+template <typename T, class S>
 cfdb_status launch_pcg(cfdb_context* ctx, PcgParams<T>& P) {
-  auto kernel = pcg_persistent<T, PY>;
+  auto kernel = pcg_persistent<T, S>;
+  const size_t smem = sizeof(T) * (size_t)S::BOX;
+  CFDB_CUDA(ctx, cudaFuncSetAttribute((const void*)kernel,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
-  CFDB_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel,
-                                                                kThreads, 0));
+  CFDB_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, smem));
   if (per_sm < 1) return set_error(ctx, CFDB_ERR_CUDA, "pcg kernel cannot be resident");
   int64_t grid = (int64_t)per_sm * ctx->num_sms;
-  grid = std::min<int64_t>(grid, P.tl.items);
+  grid = std::min<int64_t>(grid, P.cs.items);
   grid = std::max<int64_t>(grid, 1);
   cfdb_status st = ensure_partials(ctx, 4 * (size_t)grid);
   if (st != CFDB_OK) return st;
@@ -382,11 +419,69 @@ cfdb_status launch_pcg(cfdb_context* ctx, PcgParams<T>& P) {
   P.out = ctx->scalars;
   CFDB_CUDA(ctx, cudaMemsetAsync(ctx->sync_words, 0, 4 * sizeof(unsigned), ctx->stream));
   CFDB_CUDA(ctx, cudaMemsetAsync(ctx->scalars, 0, 8 * sizeof(double), ctx->stream));
-  dim3 block(kThreads / PY, PY);
+  dim3 block(kThreads);
   void* args[] = {&P};
   CFDB_CUDA(ctx, cudaEventRecord(ctx->ev_k0, ctx->stream));
   CFDB_CUDA(ctx, cudaLaunchCooperativeKernel((const void*)kernel, dim3((unsigned)grid), block, args,
-                                             0, ctx->stream));
+                                             smem, ctx->stream));
+  CFDB_CUDA(ctx, cudaEventRecord(ctx->ev_k1, ctx->stream));
+  count_launch(ctx);
+  return CFDB_OK;
+}
+
+bool getenv_flag(const char* name) {
+  const char* v = std::getenv(name);
+  return v && v[0] && v[0] != '0';
+}
+
+template <typename T, class S>
+cfdb_status launch_pcg_tma(cfdb_context* ctx, PcgParams<T>& P) {
+  TmaParams<T> TP{};
+  const CUtensorMapDataType dt = sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64
+                                                : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  const int rank = S::D3 ? 3 : 2;
+  const uint64_t dims3[3] = {(uint64_t)P.A.nx, (uint64_t)P.A.ny, (uint64_t)P.A.nz};
+  const uint64_t dims2[2] = {(uint64_t)P.A.nx, (uint64_t)P.A.nz};
+  const uint64_t* dims = S::D3 ? dims3 : dims2;
+  const uint32_t halo3[3] = {(uint32_t)S::HX, (uint32_t)S::HY, (uint32_t)S::HZ};
+  const uint32_t halo2[2] = {(uint32_t)S::HX, (uint32_t)S::HZ};
+  const uint32_t intr3[3] = {(uint32_t)S::TX, (uint32_t)S::TY, (uint32_t)S::TZ};
+  const uint32_t intr2[2] = {(uint32_t)S::TX, (uint32_t)S::TZ};
+  const uint32_t* halo = S::D3 ? halo3 : halo2;
+  const uint32_t* intr = S::D3 ? intr3 : intr2;
+  const int es = (int)sizeof(T);
+  if (!encode_tensor_map(&TP.maps.r_halo, dt, es, rank, P.r, dims, halo) ||
+      !encode_tensor_map(&TP.maps.p0_halo, dt, es, rank, P.p0, dims, halo) ||
+      !encode_tensor_map(&TP.maps.p1_halo, dt, es, rank, P.p1, dims, halo) ||
+      !encode_tensor_map(&TP.maps.x_int, dt, es, rank, P.x, dims, intr) ||
+      !encode_tensor_map(&TP.maps.r_int, dt, es, rank, P.r, dims, intr))
+    return set_error(ctx, CFDB_ERR_CUDA, "cuTensorMapEncodeTiled rejected a p' tensor map");
+  auto kernel = P.A.fx ? pcg_tma<T, S, true> : pcg_tma<T, S, false>;
+  const size_t smem = sizeof(T) * (size_t)S::STAGE * 2;
+  CFDB_CUDA(ctx, cudaFuncSetAttribute((const void*)kernel,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per_sm = 0;
+  CFDB_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kTmaThreads, smem));
+  if (per_sm < 1) return set_error(ctx, CFDB_ERR_CUDA, "TMA pcg kernel cannot be resident");
+  int64_t grid = (int64_t)per_sm * ctx->num_sms;
+  grid = std::min<int64_t>(grid, P.cs.items);
+  grid = std::max<int64_t>(grid, 1);
+  cfdb_status st = ensure_partials(ctx, 4 * (size_t)grid);
+  if (st != CFDB_OK) return st;
+  P.partials = ctx->partials;
+  P.sync.count = ctx->sync_words;
+  P.sync.gen = ctx->sync_words + 1;
+  P.sync.error = ctx->sync_words + 2;
+  P.sync.nblocks = (unsigned)grid;
+  P.sync.timeout_ns = kBarrierTimeoutNs;
+  P.out = ctx->scalars;
+  TP.P = P;
+  CFDB_CUDA(ctx, cudaMemsetAsync(ctx->sync_words, 0, 4 * sizeof(unsigned), ctx->stream));
+  CFDB_CUDA(ctx, cudaMemsetAsync(ctx->scalars, 0, 8 * sizeof(double), ctx->stream));
+  void* args[] = {&TP};
+  CFDB_CUDA(ctx, cudaEventRecord(ctx->ev_k0, ctx->stream));
+  CFDB_CUDA(ctx, cudaLaunchCooperativeKernel((const void*)kernel, dim3((unsigned)grid),
+                                             dim3(kTmaThreads), args, smem, ctx->stream));
   CFDB_CUDA(ctx, cudaEventRecord(ctx->ev_k1, ctx->stream));
   count_launch(ctx);
   return CFDB_OK;
@@ -398,6 +493,7 @@ cfdb_status run_pcg(cfdb_context* ctx, const cfdb_poperator* op, const T* b, T* 
                     double* hist_dev, int64_t hist_cap) {
   PcgParams<T> P{};
   P.A = view<T>(op);
+  if constexpr (sizeof(T) == 8) P.invd = op->invd64; else P.invd = op->invd32;
   P.b = b;
   P.x = x;
   P.r = r;
@@ -409,12 +505,20 @@ cfdb_status run_pcg(cfdb_context* ctx, const cfdb_poperator* op, const T* b, T* 
   P.max_it = max_it;
   P.hist = hist_dev;
   P.hist_cap = hist_cap;
-  if (is3d(op)) {
-    P.tl = make_tiling<32, 8>(op->knx, op->kny, op->knz);
-    return launch_pcg<T, 8>(ctx, P);
+  if (((int64_t)op->knx * (int64_t)sizeof(T)) % 16 == 0 && !getenv_flag("CFDB_NO_TMA")) {
+    if (is3d(op)) {
+      P.cs = make_split<TmaTile3D<T>>(op->knx, op->kny, op->knz);
+      return launch_pcg_tma<T, TmaTile3D<T>>(ctx, P);
+    }
+    P.cs = make_split<TmaTile2D<T>>(op->knx, op->kny, op->knz);
+    return launch_pcg_tma<T, TmaTile2D<T>>(ctx, P);
   }
-  P.tl = make_tiling<256, 1>(op->knx, op->kny, op->knz);
-  return launch_pcg<T, 1>(ctx, P);
+  if (is3d(op)) {
+    P.cs = make_split<Tile3D>(op->knx, op->kny, op->knz);
+    return launch_pcg<T, Tile3D>(ctx, P);
+  }
+  P.cs = make_split<Tile2D>(op->knx, op->kny, op->knz);
+  return launch_pcg<T, Tile2D>(ctx, P);
 }
 
 // Algorithmic bytes of one persistent PCG launch: the initial pass reads b
@@ -786,6 +890,12 @@ cfdb_status cfdb_poperator_create_faces(cfdb_context* ctx, const cfdb_grid* grid
                               cudaMemcpyHostToDevice));
     CFDB_CUDA(ctx, cudaMemcpy(op->f32[ka], f32.data(), m * sizeof(float), cudaMemcpyHostToDevice));
   }
+  CFDB_CUDA(ctx, cudaMalloc((void**)&op->invd64, sizeof(double) * (size_t)op->cells));
+  CFDB_CUDA(ctx, cudaMalloc((void**)&op->invd32, sizeof(float) * (size_t)op->cells));
+  inverse_diagonal<double><<<1024, 256, 0, ctx->stream>>>(view<double>(op), op->invd64);
+  inverse_diagonal<float><<<1024, 256, 0, ctx->stream>>>(view<float>(op), op->invd32);
+  CFDB_CHECK_LAUNCH(ctx);
+  CFDB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   *out = op;
   return CFDB_OK;
 }
@@ -801,6 +911,8 @@ void cfdb_poperator_destroy(cfdb_poperator* op) {
   for (int q = 0; q < 6; ++q) cudaFree(op->w64[q]);
   for (int q = 0; q < 5; ++q) cudaFree(op->w32[q]);
   cudaFree(op->hist_dev);
+  cudaFree(op->invd64);
+  cudaFree(op->invd32);
   delete op;
 }
 

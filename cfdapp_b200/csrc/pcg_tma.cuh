@@ -1,0 +1,442 @@
+// Persistent Jacobi-PCG with TMA-staged sweeps (included by pcg.cu).
+//
+// Same algorithm, partition and reductions as the register-staged kernel;
+// the difference is how a chunk reaches shared memory: one thread issues
+// cp.async.bulk.tensor loads of the chunk's halo box (and interior boxes)
+// into one of two stages while the block computes the other stage, and every
+// thread waits on the stage's mbarrier (bounded).  Requires the row pitch to
+// be a multiple of 16 bytes (nx even in FP64, nx % 4 == 0 in FP32); boxes
+// start 16/sizeof(T) cells left of the chunk so that x is 16-byte aligned.
+#pragma once
+
+template <typename T, int TX_, int TY_, int TZ_>
+struct TmaShape {
+  static constexpr int XO = 16 / (int)sizeof(T);
+  static constexpr bool D3 = TY_ > 1;
+  static constexpr int OY = D3 ? 1 : 0;
+  static constexpr int TX = TX_, TY = TY_, TZ = TZ_;
+  static constexpr int HX = TX + 2 * XO, HY = D3 ? TY + 2 : 1, HZ = TZ + 2;
+  static constexpr int HALO = HX * HY * HZ;
+  static constexpr int INTR = TX * TY * TZ;
+  static constexpr int pad(int elems) { return ((elems * (int)sizeof(T) + 127) / 128) * 128 / (int)sizeof(T); }
+  static constexpr int HALO_P = pad(HALO), INTR_P = pad(INTR);
+  static constexpr int STAGE = (2 * HALO_P > HALO_P + 2 * INTR_P) ? 2 * HALO_P : HALO_P + 2 * INTR_P;
+  static constexpr uint32_t BYTES_A = 2u * HALO * sizeof(T);
+  static constexpr uint32_t BYTES_B = (uint32_t)(HALO + 2 * INTR) * sizeof(T);
+};
+
+template <typename T>
+using TmaTile2D = TmaShape<T, 128, 1, 32>;
+template <typename T>
+using TmaTile3D = TmaShape<T, 32, 8, 12>;
+
+struct alignas(64) TmaMaps {
+  CUtensorMap r_halo, p0_halo, p1_halo, x_int, r_int;
+};
+
+template <typename T>
+struct TmaParams {
+  TmaMaps maps;
+  PcgParams<T> P;
+};
+
+struct ChunkIter {
+  int64_t w, w1;
+  template <int TZ>
+  __device__ __forceinline__ bool next(const ColumnSplit& cs, int nz, int tx, int ty, Chunk& c) {
+    if (w >= w1) return false;
+    const int64_t col = w / nz;
+    const int z = (int)(w % nz);
+    int64_t len = w1 - w;
+    if (len > nz - z) len = nz - z;
+    if (len > TZ) len = TZ;
+    c.i0 = (int)(col % cs.cols_x) * tx;
+    c.j0 = (int)(col / cs.cols_x) * ty;
+    c.z0 = z;
+    c.z1 = z + (int)len;
+    w += len;
+    return true;
+  }
+};
+
+
+// Per-column part of a cell's coefficients: the x/y couplings and their
+// partial diagonal sum are constant along z, so a thread walking a column
+// loads them once.  raw* keep boundary faces (they enter the diagonal),
+// c* are the couplings (zero across a boundary).
+template <typename T>
+struct ColCoef {
+  T sxy;                 // ((xl + xh) + yl) + yh, the reference's summation order
+  T cxl, cxh, cyl, cyh;  // couplings
+  bool has_ref;          // the pinned reference cell lies in this column
+  int ref_k;
+};
+
+template <typename T>
+__device__ __forceinline__ ColCoef<T> column_coef(const OpView<T>& A, int i, int j) {
+  ColCoef<T> c;
+  const T xl = __ldg(A.tx + i), xh = __ldg(A.tx + i + 1);
+  const T yl = __ldg(A.ty + j), yh = __ldg(A.ty + j + 1);
+  c.sxy = ((xl + xh) + yl) + yh;
+  c.cxl = i > 0 ? xl : T(0);
+  c.cxh = i < A.nx - 1 ? xh : T(0);
+  c.cyl = j > 0 ? yl : T(0);
+  c.cyh = j < A.ny - 1 ? yh : T(0);
+  const int64_t plane = (int64_t)A.nx * A.ny;
+  const int64_t col = i + (int64_t)A.nx * j;
+  c.has_ref = A.pinned && (A.ref % plane) == col;
+  c.ref_k = (int)(A.ref / plane);
+  return c;
+}
+
+// Coefficients of cell (i,j,k) for operators with per-face arrays.
+template <typename T>
+__device__ __forceinline__ Coef<T> face_coef(const OpView<T>& A, int i, int j, int k) {
+  return load_coef(A, i, j, k);
+}
+
+constexpr int kTmaThreads = 512;
+
+template <typename T, class S, bool FACE>
+__global__ void __launch_bounds__(kTmaThreads, 1) pcg_tma(const __grid_constant__ TmaParams<T> TP) {
+  extern __shared__ __align__(128) unsigned char smem_tma[];
+  T* stage_mem = reinterpret_cast<T*>(smem_tma);
+  __shared__ __align__(8) uint64_t bars[2];
+  __shared__ double red[64];
+  const PcgParams<T>& P = TP.P;
+  const OpView<T>& A = P.A;
+  const int B = gridDim.x, blk = blockIdx.x;
+  const int tid = threadIdx.x;
+  const bool leader = (blk == 0 && tid == 0);
+  const ColumnSplit cs = P.cs;
+  const int64_t w0 = cs.items * blk / B, w1 = cs.items * (blk + 1) / B;
+  int round = 0;
+  auto part = [&]() { return P.partials + (size_t)(round & 1) * 2 * B; };
+  if (tid == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  uint32_t parity[2] = {0u, 0u};
+
+  auto idx_of = [&](int i, int j, int k) { return i + (int64_t)A.nx * (j + (int64_t)A.ny * k); };
+
+  // Generic pipelined sweep: load(c, base, bar) issues the chunk's TMA copies
+  // (thread 0), body(c, base) computes it.  Returns false on a failed wait.
+  auto pipeline = [&](auto load, auto body) -> bool {
+    ChunkIter ld{w0, w1}, cp{w0, w1};
+    Chunk cl, cc;
+    if (ld.template next<S::TZ>(cs, A.nz, S::TX, S::TY, cl) && tid == 0)
+      load(cl, stage_mem, &bars[0]);
+    int q = 0;
+    while (cp.template next<S::TZ>(cs, A.nz, S::TX, S::TY, cc)) {
+      const int st = q & 1;
+      Chunk cn;
+      if (ld.template next<S::TZ>(cs, A.nz, S::TX, S::TY, cn) && tid == 0)
+        load(cn, stage_mem + (size_t)(st ^ 1) * S::STAGE, &bars[st ^ 1]);
+      const bool ok = mbar_wait(&bars[st], parity[st], P.sync.error, P.sync.timeout_ns);
+      parity[st] ^= 1u;
+      if (__syncthreads_or(!ok)) return false;
+      body(cc, stage_mem + (size_t)st * S::STAGE);
+      __syncthreads();
+      ++q;
+    }
+    return true;
+  };
+
+  // ---- r0 = b - A x0 (plain loads: once per solve), ||r0||^2, r0.z0
+  double acc[2] = {0.0, 0.0};
+  {
+    ChunkIter cp{w0, w1};
+    Chunk c;
+    while (cp.template next<S::TZ>(cs, A.nz, S::TX, S::TY, c)) {
+      const int n = S::TX * S::TY * (c.z1 - c.z0);
+      for (int q = tid; q < n; q += kTmaThreads) {
+        const int i = c.i0 + q % S::TX, j = c.j0 + (q / S::TX) % S::TY, k = c.z0 + q / (S::TX * S::TY);
+        if (i >= A.nx || j >= A.ny) continue;
+        const int64_t idx = idx_of(i, j, k);
+        const Coef<T> cf = load_coef(A, i, j, k);
+        T rn = __ldg(P.b + idx);
+        if (!P.x0_zero) {
+          auto xv = [&](int ii, int jj, int kk) {
+            return (ii >= 0 && ii < A.nx && jj >= 0 && jj < A.ny && kk >= 0 && kk < A.nz)
+                       ? P.x[idx_of(ii, jj, kk)] : T(0);
+          };
+          rn = rn - apply_coef(cf, P.x[idx], xv(i - 1, j, k), xv(i + 1, j, k), xv(i, j - 1, k),
+                               xv(i, j + 1, k), xv(i, j, k - 1), xv(i, j, k + 1));
+        }
+        P.r[idx] = rn;
+        const double rd = (double)rn;
+        acc[0] += rd * rd;
+        acc[1] += rd * (double)(cf.inv * rn);
+      }
+    }
+  }
+  block_sum<2>(acc, red);
+  if (tid == 0) {
+    part()[2 * blk] = acc[0];
+    part()[2 * blk + 1] = acc[1];
+  }
+  if (!grid_sync(P.sync)) return;
+  double tot[2];
+  grid_total<2>(part(), 2, B, tot, red);
+  ++round;
+  const double b0 = sqrt(tot[0]);
+  double rz = tot[1];
+  auto converged = [&](double res) {
+    return (res <= P.abs_tol) || ((b0 > 0.0) && (res / b0 <= P.rel_tol));
+  };
+  if (leader) {
+    P.out[OUT_B0] = b0;
+    if (P.hist_cap > 0) P.hist[0] = b0;
+  }
+  if (b0 == 0.0 || converged(b0) || !finite(rz)) {
+    if (leader) {
+      P.out[OUT_STATUS] = (b0 == 0.0 || converged(b0)) ? CFDB_SOLVER_CONVERGED : CFDB_SOLVER_BREAKDOWN;
+      P.out[OUT_ITER] = 0;
+      P.out[OUT_FINAL] = b0;
+    }
+    return;
+  }
+
+  double res_cur = b0;
+  double beta = 0.0;
+  bool pold_is_p0 = true;
+  for (int64_t it = 1; it <= P.max_it; ++it) {
+    const bool first = (it == 1);
+    const T tbeta = (T)beta;
+    const CUtensorMap* pold_map = pold_is_p0 ? &TP.maps.p0_halo : &TP.maps.p1_halo;
+    const CUtensorMap* pnew_map = pold_is_p0 ? &TP.maps.p1_halo : &TP.maps.p0_halo;
+    T* pnew = pold_is_p0 ? P.p1 : P.p0;
+    // ---- sweep A: stage r, p_old halo boxes; p = D^-1 r + beta p_old; Ap; p.Ap
+    double pap = 0.0;
+    const bool okA = pipeline(
+        [&](const Chunk& c, T* base, uint64_t* bar) {
+          fence_proxy_async_smem();
+          mbar_arrive_expect_tx(bar, S::BYTES_A);
+          const int hx = c.i0 - S::XO, hy = c.j0 - S::OY, hz = c.z0 - 1;
+          if constexpr (S::D3) {
+            tma_load_3d(base, &TP.maps.r_halo, hx, hy, hz, bar);
+            tma_load_3d(base + S::HALO_P, pold_map, hx, hy, hz, bar);
+          } else {
+            tma_load_2d(base, &TP.maps.r_halo, hx, hz, bar);
+            tma_load_2d(base + S::HALO_P, pold_map, hx, hz, bar);
+          }
+        },
+        [&](const Chunk& c, T* base) {
+          T* rb = base;
+          const T* pb = base + S::HALO_P;
+          const int zl = c.z1 - c.z0;
+          constexpr int PL = S::HX * S::HY;  // box plane stride
+          // transform p = D^-1 r + beta p_old over the used halo elements
+          // (columns XO-1 .. XO+TX of the box), evenly over the threads
+          constexpr int UX = S::TX + 2;
+          const int nuse = UX * S::HY * (zl + 2);
+          for (int u = tid; u < nuse; u += kTmaThreads) {
+            const int cx = u % UX;
+            const int rest = u / UX;
+            const int cy = rest % S::HY, kk = rest / S::HY - 1;
+            const int i = c.i0 - 1 + cx, j = c.j0 - S::OY + cy, k = c.z0 + kk;
+            if (i < 0 || i >= A.nx || j < 0 || j >= A.ny || k < 0 || k >= A.nz) continue;
+            const int e = (cx + S::XO - 1) + S::HX * cy + PL * (kk + 1);
+            T inv;
+            if constexpr (FACE) {
+              inv = __ldg(P.invd + (i + (int64_t)A.nx * (j + (int64_t)A.ny * k)));
+            } else {
+              const T sxy = ((__ldg(A.tx + i) + __ldg(A.tx + i + 1)) + __ldg(A.ty + j)) + __ldg(A.ty + j + 1);
+              const T dg = (sxy + __ldg(A.tz + k)) + __ldg(A.tz + k + 1);
+              const bool pin = A.pinned && (i + (int64_t)A.nx * (j + (int64_t)A.ny * k)) == A.ref;
+              inv = pin ? T(1) : rcp_rn(dg);
+            }
+            const T z = inv * rb[e];
+            rb[e] = first ? z : fma(tbeta, pb[e], z);
+          }
+          __syncthreads();
+          // interior: Ap, store p, p.Ap -- one thread per column (x fastest)
+          constexpr int ICOL = S::TX * S::TY;
+          constexpr int SPLIT = kTmaThreads / ICOL > 0 ? kTmaThreads / ICOL : 1;
+          for (int t = tid; t < ICOL * SPLIT; t += kTmaThreads) {
+            const int col = t % ICOL, part_z = t / ICOL;
+            const int qx = col % S::TX, qy = col / S::TX;
+            const int i = c.i0 + qx, j = c.j0 + qy;
+            if (i >= A.nx || j >= A.ny) continue;
+            const int kb = zl * part_z / SPLIT, ke = zl * (part_z + 1) / SPLIT;
+            int e = (qx + S::XO) + S::HX * (qy + S::OY) + PL * (kb + 1);
+            int64_t idx = i + (int64_t)A.nx * (j + (int64_t)A.ny * (c.z0 + kb));
+            const int64_t pstride = (int64_t)A.nx * A.ny;
+            if constexpr (FACE) {
+              for (int kk = kb; kk < ke; ++kk, e += PL, idx += pstride) {
+                const Coef<T> cf = face_coef(A, i, j, c.z0 + kk);
+                const T v = rb[e];
+                const T ap = apply_coef(cf, v, rb[e - 1], rb[e + 1], S::D3 ? rb[e - S::HX] : T(0),
+                                        S::D3 ? rb[e + S::HX] : T(0), rb[e - PL], rb[e + PL]);
+                pnew[idx] = v;
+                pap += (double)v * (double)ap;
+              }
+            } else {
+              const ColCoef<T> cc = column_coef(A, i, j);
+              for (int kk = kb; kk < ke; ++kk, e += PL, idx += pstride) {
+                const int k = c.z0 + kk;
+                const T zl_ = __ldg(A.tz + k), zh_ = __ldg(A.tz + k + 1);
+                const T v = rb[e];
+                T ap;
+                if (cc.has_ref && k == cc.ref_k) {
+                  ap = v;
+                } else {
+                  const T dg = (cc.sxy + zl_) + zh_;
+                  T off = cc.cxl * rb[e - 1];
+                  off = fma(cc.cxh, rb[e + 1], off);
+                  if (S::D3) {
+                    off = fma(cc.cyl, rb[e - S::HX], off);
+                    off = fma(cc.cyh, rb[e + S::HX], off);
+                  }
+                  off = fma(k > 0 ? zl_ : T(0), rb[e - PL], off);
+                  off = fma(k < A.nz - 1 ? zh_ : T(0), rb[e + PL], off);
+                  ap = fma(dg, v, -off);
+                }
+                pnew[idx] = v;
+                pap += (double)v * (double)ap;
+              }
+            }
+          }
+        });
+    {
+      double a1[1] = {pap};
+      block_sum<1>(a1, red);
+      if (tid == 0) part()[2 * blk] = a1[0];
+    }
+    if (!okA || !grid_sync(P.sync)) return;
+    double t1[1];
+    grid_total<1>(part(), 2, B, t1, red);
+    ++round;
+    const double pAp = t1[0];
+    const double alpha = rz / pAp;
+    if (!finite(pAp) || fabs(pAp) < 1.0e-30 || !finite(alpha)) {
+      if (leader) {
+        P.out[OUT_STATUS] = CFDB_SOLVER_BREAKDOWN;
+        P.out[OUT_ITER] = (double)(it - 1);
+        P.out[OUT_FINAL] = res_cur;
+      }
+      return;
+    }
+    const T talpha = (T)alpha;
+    // ---- sweep B: stage p halo, x and r interiors; x += alpha p; r -= alpha A p
+    double ab[2] = {0.0, 0.0};
+    const bool okB = pipeline(
+        [&](const Chunk& c, T* base, uint64_t* bar) {
+          fence_proxy_async_smem();
+          mbar_arrive_expect_tx(bar, S::BYTES_B);
+          const int hx = c.i0 - S::XO, hy = c.j0 - S::OY, hz = c.z0 - 1;
+          if constexpr (S::D3) {
+            tma_load_3d(base, pnew_map, hx, hy, hz, bar);
+            tma_load_3d(base + S::HALO_P, &TP.maps.x_int, c.i0, c.j0, c.z0, bar);
+            tma_load_3d(base + S::HALO_P + S::INTR_P, &TP.maps.r_int, c.i0, c.j0, c.z0, bar);
+          } else {
+            tma_load_2d(base, pnew_map, hx, hz, bar);
+            tma_load_2d(base + S::HALO_P, &TP.maps.x_int, c.i0, c.z0, bar);
+            tma_load_2d(base + S::HALO_P + S::INTR_P, &TP.maps.r_int, c.i0, c.z0, bar);
+          }
+        },
+        [&](const Chunk& c, T* base) {
+          const T* pb = base;
+          const T* xb = base + S::HALO_P;
+          const T* rb = base + S::HALO_P + S::INTR_P;
+          const int zl = c.z1 - c.z0;
+          constexpr int PL = S::HX * S::HY;
+          constexpr int IPL = S::TX * S::TY;
+          constexpr int ICOL = S::TX * S::TY;
+          constexpr int SPLIT = kTmaThreads / ICOL > 0 ? kTmaThreads / ICOL : 1;
+          for (int t = tid; t < ICOL * SPLIT; t += kTmaThreads) {
+            const int col = t % ICOL, part_z = t / ICOL;
+            const int qx = col % S::TX, qy = col / S::TX;
+            const int i = c.i0 + qx, j = c.j0 + qy;
+            if (i >= A.nx || j >= A.ny) continue;
+            const int kb = zl * part_z / SPLIT, ke = zl * (part_z + 1) / SPLIT;
+            int e = (qx + S::XO) + S::HX * (qy + S::OY) + PL * (kb + 1);
+            int q = col + IPL * kb;
+            int64_t idx = i + (int64_t)A.nx * (j + (int64_t)A.ny * (c.z0 + kb));
+            const int64_t pstride = (int64_t)A.nx * A.ny;
+            ColCoef<T> cc;
+            if constexpr (!FACE) cc = column_coef(A, i, j);
+            for (int kk = kb; kk < ke; ++kk, e += PL, q += IPL, idx += pstride) {
+              const int k = c.z0 + kk;
+              const T v = pb[e];
+              T ap, inv;
+              if constexpr (FACE) {
+                const Coef<T> cf = face_coef(A, i, j, k);
+                ap = apply_coef(cf, v, pb[e - 1], pb[e + 1], S::D3 ? pb[e - S::HX] : T(0),
+                                S::D3 ? pb[e + S::HX] : T(0), pb[e - PL], pb[e + PL]);
+                inv = __ldg(P.invd + idx);
+              } else if (cc.has_ref && k == cc.ref_k) {
+                ap = v;
+                inv = T(1);
+              } else {
+                const T zl_ = __ldg(A.tz + k), zh_ = __ldg(A.tz + k + 1);
+                const T dg = (cc.sxy + zl_) + zh_;
+                T off = cc.cxl * pb[e - 1];
+                off = fma(cc.cxh, pb[e + 1], off);
+                if (S::D3) {
+                  off = fma(cc.cyl, pb[e - S::HX], off);
+                  off = fma(cc.cyh, pb[e + S::HX], off);
+                }
+                off = fma(k > 0 ? zl_ : T(0), pb[e - PL], off);
+                off = fma(k < A.nz - 1 ? zh_ : T(0), pb[e + PL], off);
+                ap = fma(dg, v, -off);
+                inv = rcp_rn(dg);
+              }
+              P.x[idx] = fma(talpha, v, xb[q]);
+              const T rn = fma(-talpha, ap, rb[q]);
+              P.r[idx] = rn;
+              const double rd = (double)rn;
+              ab[0] += rd * rd;
+              ab[1] += rd * (double)(inv * rn);
+            }
+          }
+        });
+    block_sum<2>(ab, red);
+    if (tid == 0) {
+      part()[2 * blk] = ab[0];
+      part()[2 * blk + 1] = ab[1];
+    }
+    if (!okB || !grid_sync(P.sync)) return;
+    grid_total<2>(part(), 2, B, tot, red);
+    ++round;
+    const double res = sqrt(tot[0]);
+    if (leader && it < P.hist_cap) P.hist[it] = res;
+    if (!finite(res)) {
+      if (leader) {
+        P.out[OUT_STATUS] = CFDB_SOLVER_NONFINITE_RESIDUAL;
+        P.out[OUT_ITER] = (double)it;
+        P.out[OUT_FINAL] = res;
+      }
+      return;
+    }
+    res_cur = res;
+    if (converged(res)) {
+      if (leader) {
+        P.out[OUT_STATUS] = CFDB_SOLVER_CONVERGED;
+        P.out[OUT_ITER] = (double)it;
+        P.out[OUT_FINAL] = res;
+      }
+      return;
+    }
+    const double rzNew = tot[1];
+    beta = rzNew / rz;
+    if (!finite(rzNew) || !finite(beta)) {
+      if (leader) {
+        P.out[OUT_STATUS] = CFDB_SOLVER_BREAKDOWN;
+        P.out[OUT_ITER] = (double)it;
+        P.out[OUT_FINAL] = res;
+      }
+      return;
+    }
+    rz = rzNew;
+    pold_is_p0 = !pold_is_p0;
+  }
+  if (leader) {
+    P.out[OUT_STATUS] = CFDB_SOLVER_MAX_ITERATIONS;
+    P.out[OUT_ITER] = (double)P.max_it;
+    P.out[OUT_FINAL] = res_cur;
+  }
+}

@@ -40,6 +40,10 @@ struct Coef {
   T diag, inv;               // diagonal (face-order sum incl. Dirichlet faces) and 1/diag
 };
 
+// Correctly rounded reciprocal (== 1/x in IEEE round-to-nearest).
+__device__ __forceinline__ double rcp_rn(double x) { return __drcp_rn(x); }
+__device__ __forceinline__ float rcp_rn(float x) { return __frcp_rn(x); }
+
 template <typename T>
 __device__ __forceinline__ Coef<T> load_coef(const OpView<T>& A, int i, int j, int k) {
   Coef<T> c;
@@ -77,7 +81,7 @@ __device__ __forceinline__ Coef<T> load_coef(const OpView<T>& A, int i, int j, i
   // The reference sums the diagonal in face order: x-low, x-high, y-low,
   // y-high, z-low, z-high (PressureCorrectionEquation.cpp:266-298).
   c.diag = ((((c.xl + c.xh) + c.yl) + c.yh) + c.zl) + c.zh;
-  c.inv = T(1) / c.diag;
+  c.inv = rcp_rn(c.diag);
   if (i == 0) c.xl = T(0);
   if (i == A.nx - 1) c.xh = T(0);
   if (j == 0) c.yl = T(0);
@@ -148,8 +152,11 @@ __device__ __forceinline__ void march(const OpView<T>& A, const Tiling& tl, int6
     __syncthreads();
     if (act) {
       const int64_t idx = i + (int64_t)A.nx * (j + (int64_t)A.ny * k);
-      cell(i, j, k, idx, vcur, s[ty + 1][tx], s[ty + 1][tx + 2], s[ty][tx + 1], s[ty + 2][tx + 1],
-           vprev, vnext);
+      // With a single row of threads (PY == 1, the 2D layout) the y-halo rows
+      // of the plane buffer are never written: pass zeros, not stale memory.
+      const T vs = (PY > 1) ? s[ty][tx + 1] : T(0);
+      const T vn = (PY > 1) ? s[ty + 2][tx + 1] : T(0);
+      cell(i, j, k, idx, vcur, s[ty + 1][tx], s[ty + 1][tx + 2], vs, vn, vprev, vnext);
     }
     vprev = vcur;
     vcur = vnext;
