@@ -332,3 +332,247 @@ class POperator:
             self.close()
         except Exception:
             pass
+
+
+# ------------------------------------------------------------------ SIMPLE
+VBC = {"wall": 0, "moving_wall": 1, "inlet": 2, "outlet": 3}
+PBC = {"fixed_gradient": 0, "fixed_value": 1}
+SCHEME = {"upwind": 0, "central": 1, "linear_upwind": 2, "lud": 2, "quick": 3}
+FACE_FLUX = {"linear": 0, "rhie_chow": 1, "rhiechow": 1, "automatic": 2, "auto": 2}
+
+
+class _SimpleCase(C.Structure):
+    _fields_ = [("grid", _Grid), ("vbc_type", C.c_int * 6), ("vbc_value", (C.c_double * 3) * 6),
+                ("pbc_type", C.c_int * 6), ("pbc_value", C.c_double * 6), ("rho", C.c_double),
+                ("mu", C.c_double)]
+
+
+class _SimpleSettings(C.Structure):
+    _fields_ = [("max_outer", C.c_int64), ("alpha_u", C.c_double), ("alpha_p", C.c_double),
+                ("tol_u", C.c_double), ("tol_p", C.c_double), ("tol_c", C.c_double),
+                ("scheme", C.c_int), ("face_flux", C.c_int), ("reference_cell", C.c_int64),
+                ("momentum", _LinSettings), ("pressure", _LinSettings)]
+
+
+class _SimpleResult(C.Structure):
+    _fields_ = [("status", C.c_int), ("iterations", C.c_int64), ("final_u", C.c_double),
+                ("final_v", C.c_double), ("final_w", C.c_double), ("final_p", C.c_double),
+                ("final_continuity", C.c_double), ("global_imbalance", C.c_double),
+                ("momentum_linear_iterations", C.c_int64),
+                ("pressure_linear_iterations", C.c_int64), ("device_ms", C.c_double),
+                ("pressure_solve_ms", C.c_double), ("momentum_solve_ms", C.c_double),
+                ("kernel_launches", C.c_int64)]
+
+
+@dataclass
+class SimpleCase:
+    """A uniform Cartesian case (MeshGeometry::createCartesian2D/3D + BCs + fluid)."""
+    dim: int
+    n: tuple
+    length: tuple = (1.0, 1.0, 1.0)
+    vbc: tuple = ()     # per patch: (type, (vx, vy, vz))
+    pbc: tuple = ()     # per patch: (type, value)
+    rho: float = 1.0
+    mu: float = 0.01
+
+    @staticmethod
+    def cavity(dim: int, n: int, lid: float = 1.0, mu: float = 0.01, rho: float = 1.0):
+        vbc = [("wall", (0.0, 0.0, 0.0))] * (2 * dim)
+        vbc[3] = ("moving_wall", (lid, 0.0, 0.0))
+        return SimpleCase(dim, (n,) * dim, (1.0, 1.0, 1.0), tuple(vbc),
+                          tuple([("fixed_gradient", 0.0)] * (2 * dim)), rho, mu)
+
+    @staticmethod
+    def channel(nx: int, ny: int, lx: float, ly: float, inlet: float = 1.0, mu: float = 0.1,
+                rho: float = 1.0):
+        vbc = (("inlet", (inlet, 0.0, 0.0)), ("outlet", (0.0, 0.0, 0.0)),
+               ("wall", (0.0, 0.0, 0.0)), ("wall", (0.0, 0.0, 0.0)))
+        pbc = (("fixed_gradient", 0.0), ("fixed_value", 0.0), ("fixed_gradient", 0.0),
+               ("fixed_gradient", 0.0))
+        return SimpleCase(2, (nx, ny), (lx, ly, 1.0), vbc, pbc, rho, mu)
+
+    def cells(self) -> int:
+        return int(np.prod(self.n[: self.dim]))
+
+    def faces(self) -> int:
+        n = list(self.n) + [1, 1]
+        nx, ny, nz = n[0], n[1], (n[2] if self.dim == 3 else 1)
+        f = (nx + 1) * ny * nz + nx * (ny + 1) * nz
+        return f + (nx * ny * (nz + 1) if self.dim == 3 else 0)
+
+    def c(self) -> _SimpleCase:
+        cs = _SimpleCase()
+        cs.grid = grid(self.dim, self.n, self.length)
+        for q in range(6):
+            t, val = self.vbc[q] if q < len(self.vbc) else ("wall", (0, 0, 0))
+            cs.vbc_type[q] = VBC[t]
+            for k in range(3):
+                cs.vbc_value[q][k] = float(val[k]) if k < len(val) else 0.0
+            pt, pv = self.pbc[q] if q < len(self.pbc) else ("fixed_gradient", 0.0)
+            cs.pbc_type[q] = PBC[pt]
+            cs.pbc_value[q] = float(pv)
+        cs.rho = self.rho
+        cs.mu = self.mu
+        return cs
+
+
+@dataclass
+class SIMPLESettings:
+    """SIMPLESettings (include/cfd/pressure_velocity/SIMPLESettings.hpp:42-145)."""
+    max_iterations: int = 1000
+    velocity_relaxation: float = 0.7
+    pressure_relaxation: float = 0.3
+    velocity_tolerance: float = 1e-8
+    pressure_tolerance: float = 1e-8
+    continuity_tolerance: float = 1e-8
+    convection_scheme: str = "upwind"
+    face_flux: str = "automatic"
+    reference_cell: int = 0
+    momentum_solver: LinearSolverSettings = None
+    pressure_solver: LinearSolverSettings = None
+
+    def __post_init__(self):
+        if self.momentum_solver is None:
+            self.momentum_solver = LinearSolverSettings(type="bicgstab", preconditioner="none")
+        if self.pressure_solver is None:
+            self.pressure_solver = LinearSolverSettings(type="bicgstab", preconditioner="none")
+
+    def c(self) -> _SimpleSettings:
+        return _SimpleSettings(self.max_iterations, self.velocity_relaxation,
+                               self.pressure_relaxation, self.velocity_tolerance,
+                               self.pressure_tolerance, self.continuity_tolerance,
+                               SCHEME[self.convection_scheme], FACE_FLUX[self.face_flux],
+                               self.reference_cell, self.momentum_solver.c(),
+                               self.pressure_solver.c())
+
+
+@dataclass
+class SIMPLEResult:
+    """SIMPLEResult (include/cfd/pressure_velocity/SIMPLEResult.hpp:80-200)."""
+    status: str
+    iterations: int
+    final: dict
+    momentum_linear_iterations: int
+    pressure_linear_iterations: int
+    device_ms: float
+    pressure_solve_ms: float
+    momentum_solve_ms: float
+    kernel_launches: int
+    u: np.ndarray
+    v: np.ndarray
+    w: np.ndarray
+    p: np.ndarray
+    flux: np.ndarray
+    history: np.ndarray
+
+    def converged(self) -> bool:
+        return self.status == "Converged"
+
+
+def _simple_sigs(L):
+    vp = C.c_void_p
+    dp = C.POINTER(C.c_double)
+    L.cfdb_simple_solve.argtypes = [vp, C.POINTER(_SimpleCase), C.POINTER(_SimpleSettings), dp, dp,
+                                    dp, dp, dp, dp, C.POINTER(_SimpleResult)]
+    L.cfdb_simple_create.argtypes = [vp, C.POINTER(_SimpleCase), C.POINTER(_SimpleSettings),
+                                     C.POINTER(vp)]
+    L.cfdb_simple_destroy.argtypes = [vp]
+    L.cfdb_simple_destroy.restype = None
+    L.cfdb_simple_set_state.argtypes = [vp, dp, dp, dp, dp]
+    L.cfdb_simple_get_state.argtypes = [vp, dp, dp, dp, dp, dp]
+    L.cfdb_simple_pressure_gradient.argtypes = [vp, dp, dp, dp]
+    L.cfdb_simple_assemble_momentum.argtypes = [vp, C.c_int, dp, C.POINTER(dp), dp]
+    L.cfdb_simple_iterate.argtypes = [vp, C.c_int64, dp, C.POINTER(_SimpleResult)]
+
+
+def _result(r: _SimpleResult, case, u, v, w, p, flux, hist) -> SIMPLEResult:
+    final = dict(u=r.final_u, v=r.final_v, w=r.final_w, p=r.final_p,
+                 continuity=r.final_continuity, global_imbalance=r.global_imbalance)
+    return SIMPLEResult(SIMPLE_STATUS[r.status], r.iterations, final, r.momentum_linear_iterations,
+                        r.pressure_linear_iterations, r.device_ms, r.pressure_solve_ms,
+                        r.momentum_solve_ms, r.kernel_launches, u, v,
+                        w if case.dim == 3 else np.zeros(0), p, flux,
+                        hist[: 5 * r.iterations].reshape(-1, 5))
+
+
+def simple_solve(ctx: Context, case: SimpleCase, settings: SIMPLESettings, u0=None, v0=None,
+                 w0=None, p0=None) -> SIMPLEResult:
+    """SIMPLE::solve on the device from host fields (zero fields by default)."""
+    L = ctx.lib
+    _simple_sigs(L)
+    n = case.cells()
+    u = np.zeros(n) if u0 is None else np.array(u0, dtype=np.float64)
+    v = np.zeros(n) if v0 is None else np.array(v0, dtype=np.float64)
+    w = np.zeros(n) if w0 is None else np.array(w0, dtype=np.float64)
+    p = np.zeros(n) if p0 is None else np.array(p0, dtype=np.float64)
+    flux = np.zeros(case.faces())
+    hist = np.zeros(5 * max(settings.max_iterations, 1))
+    r = _SimpleResult()
+    ctx.check(L.cfdb_simple_solve(ctx.handle, C.byref(case.c()), C.byref(settings.c()), _dp(u),
+                                  _dp(v), _dp(w), _dp(p), _dp(flux), _dp(hist), C.byref(r)),
+              "cfdb_simple_solve")
+    return _result(r, case, u, v, w, p, flux, hist)
+
+
+class Simple:
+    """Stage-level SIMPLE session (GpuSimpleDiscretization-like)."""
+
+    def __init__(self, ctx: Context, case: SimpleCase, settings: SIMPLESettings):
+        self.ctx, self.case, self.settings = ctx, case, settings
+        _simple_sigs(ctx.lib)
+        h = C.c_void_p()
+        ctx.check(ctx.lib.cfdb_simple_create(ctx.handle, C.byref(case.c()), C.byref(settings.c()),
+                                             C.byref(h)), "cfdb_simple_create")
+        self._h = h
+
+    def set_state(self, u, v, w, p):
+        n = self.case.cells()
+        arr = [np.ascontiguousarray(a if a is not None else np.zeros(n), dtype=np.float64)
+               for a in (u, v, w, p)]
+        self._keep = arr
+        self.ctx.check(self.ctx.lib.cfdb_simple_set_state(self._h, *[_dp(a) for a in arr]),
+                       "cfdb_simple_set_state")
+
+    def get_state(self):
+        n = self.case.cells()
+        u, v, w, p = (np.zeros(n) for _ in range(4))
+        f = np.zeros(self.case.faces())
+        self.ctx.check(self.ctx.lib.cfdb_simple_get_state(self._h, _dp(u), _dp(v), _dp(w), _dp(p),
+                                                          _dp(f)), "cfdb_simple_get_state")
+        return u, v, (w if self.case.dim == 3 else np.zeros(0)), p, f
+
+    def pressure_gradient(self):
+        n = self.case.cells()
+        g = [np.zeros(n) for _ in range(3)]
+        self.ctx.check(self.ctx.lib.cfdb_simple_pressure_gradient(self._h, *[_dp(a) for a in g]),
+                       "cfdb_simple_pressure_gradient")
+        return g[: self.case.dim]
+
+    def assemble_momentum(self, comp: int):
+        n = self.case.cells()
+        diag, rhs = np.zeros(n), np.zeros(n)
+        off = [np.zeros(n) for _ in range(6)]
+        offp = (C.POINTER(C.c_double) * 6)(*[_dp(o) for o in off])
+        self.ctx.check(self.ctx.lib.cfdb_simple_assemble_momentum(self._h, comp, _dp(diag), offp,
+                                                                  _dp(rhs)),
+                       "cfdb_simple_assemble_momentum")
+        return diag, off, rhs
+
+    def iterate(self, n: int) -> SIMPLEResult:
+        hist = np.zeros(5 * max(n, 1))
+        r = _SimpleResult()
+        self.ctx.check(self.ctx.lib.cfdb_simple_iterate(self._h, n, _dp(hist), C.byref(r)),
+                       "cfdb_simple_iterate")
+        u, v, w, p, f = self.get_state()
+        return _result(r, self.case, u, v, w, p, f, hist)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.ctx.lib.cfdb_simple_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -51,6 +51,7 @@ struct cfdb_poperator {
   int64_t hist_cap = 0;
   double* invd64 = nullptr;  // 1/diag, face-coefficient operators only
   float* invd32 = nullptr;
+  bool faces_borrowed = false;  // f64[] point into a caller's device array
 };
 
 namespace cfdb {
@@ -824,7 +825,44 @@ cfdb_status new_operator(cfdb_context* ctx, const cfdb_grid* grid, int pinned, i
   return CFDB_OK;
 }
 
+__global__ void k_to_f32(const double* in, float* out, int64_t n) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n;
+       q += (int64_t)gridDim.x * blockDim.x)
+    out[q] = (float)in[q];
+}
+
 }  // namespace
+
+// Points the operator's face coefficients at a device array in global face
+// order (x-, y-, z-faces) and refreshes the inverse diagonal (and FP32
+// copies when `fp32`).  The array must outlive the operator's next solves.
+cfdb_status poperator_bind_faces(cfdb_context* ctx, cfdb_poperator* op, const double* D, bool fp32) {
+  const cfdb_grid& g = op->grid;
+  const int64_t nx = g.n[0], ny = g.n[1], nz = g.dim == 3 ? g.n[2] : 1;
+  const int64_t nfx = (nx + 1) * ny * nz, nfy = nx * (ny + 1) * nz;
+  const int64_t counts[3] = {nfx, nfy, g.dim == 3 ? nx * ny * (nz + 1) : 0};
+  const int64_t offs[3] = {0, nfx, nfx + nfy};
+  const int kaxis[3] = {0, g.dim == 2 ? 2 : 1, 2};
+  op->faces_borrowed = true;
+  for (int a = 0; a < g.dim; ++a) {
+    const int ka = kaxis[a];
+    op->f64[ka] = const_cast<double*>(D + offs[a]);
+    if (fp32) {
+      if (!op->f32[ka]) CFDB_CUDA(ctx, cudaMalloc((void**)&op->f32[ka], sizeof(float) * counts[a]));
+      k_to_f32<<<1024, 256, 0, ctx->stream>>>(D + offs[a], op->f32[ka], counts[a]);
+    }
+  }
+  if (!op->invd64) CFDB_CUDA(ctx, cudaMalloc((void**)&op->invd64, sizeof(double) * (size_t)op->cells));
+  inverse_diagonal<double><<<1024, 256, 0, ctx->stream>>>(view<double>(op), op->invd64);
+  if (fp32) {
+    if (!op->invd32) CFDB_CUDA(ctx, cudaMalloc((void**)&op->invd32, sizeof(float) * (size_t)op->cells));
+    inverse_diagonal<float><<<1024, 256, 0, ctx->stream>>>(view<float>(op), op->invd32);
+  }
+  CFDB_CHECK_LAUNCH(ctx);
+  count_launch(ctx, fp32 ? 2 + g.dim : 1);
+  return CFDB_OK;
+}
+
 }  // namespace cfdb
 
 using namespace cfdb;
@@ -905,7 +943,7 @@ void cfdb_poperator_destroy(cfdb_poperator* op) {
   for (int q = 0; q < 3; ++q) {
     cudaFree(op->t64[q]);
     cudaFree(op->t32[q]);
-    cudaFree(op->f64[q]);
+    if (!op->faces_borrowed) cudaFree(op->f64[q]);
     cudaFree(op->f32[q]);
   }
   for (int q = 0; q < 6; ++q) cudaFree(op->w64[q]);

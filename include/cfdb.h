@@ -185,6 +185,91 @@ CFDB_API cfdb_status cfdb_copy_to_host(cfdb_context* ctx, void* dst_host, const 
 CFDB_API cfdb_status cfdb_memset_device(cfdb_context* ctx, void* dst_dev, int value, size_t bytes);
 CFDB_API cfdb_status cfdb_synchronize(cfdb_context* ctx);
 
+/* ------------------------------------------------------------------ SIMPLE */
+
+/* Velocity and pressure boundary conditions per patch (reference classes
+ * src/boundary/{Wall,MovingWall,Inlet,Outlet,FixedGradient,FixedValue}.cpp). */
+enum { CFDB_VBC_WALL = 0, CFDB_VBC_MOVING_WALL = 1, CFDB_VBC_INLET = 2, CFDB_VBC_OUTLET = 3 };
+enum { CFDB_PBC_FIXED_GRADIENT = 0, CFDB_PBC_FIXED_VALUE = 1 };
+/* ConvectionScheme (include/cfd/discretization/Convection.hpp:22-27). */
+enum { CFDB_SCHEME_UPWIND = 0, CFDB_SCHEME_CENTRAL = 1, CFDB_SCHEME_LINEAR_UPWIND = 2,
+       CFDB_SCHEME_QUICK = 3 };
+/* FaceFluxScheme (SIMPLESettings.hpp), resolved: Automatic is Linear in 2D,
+ * RhieChow in 3D (resolveFaceFluxScheme). */
+enum { CFDB_FLUX_LINEAR = 0, CFDB_FLUX_RHIE_CHOW = 1, CFDB_FLUX_AUTOMATIC = 2 };
+
+/* A laminar incompressible case on a uniform Cartesian grid: the mesh of
+ * MeshGeometry::createCartesian2D/3D, one BC per patch, constant rho, mu. */
+typedef struct {
+  cfdb_grid grid;
+  int vbc_type[6];
+  double vbc_value[6][3];
+  int pbc_type[6];
+  double pbc_value[6];
+  double rho, mu;
+} cfdb_simple_case;
+
+/* SIMPLESettings (include/cfd/pressure_velocity/SIMPLESettings.hpp:42-145),
+ * the subset this path supports (absolute convergence criterion, no
+ * non-orthogonal corrections, Green-Gauss gradients). */
+typedef struct {
+  int64_t max_outer;
+  double alpha_u, alpha_p;
+  double tol_u, tol_p, tol_c;
+  int scheme;             /* CFDB_SCHEME_* */
+  int face_flux;          /* CFDB_FLUX_* */
+  int64_t reference_cell;
+  cfdb_linear_settings momentum;
+  cfdb_linear_settings pressure;
+} cfdb_simple_settings;
+
+/* SIMPLEResult (SIMPLEResult.hpp:80-200), scalar part. */
+typedef struct {
+  int status;             /* CFDB_SIMPLE_* */
+  int64_t iterations;
+  double final_u, final_v, final_w, final_p, final_continuity, global_imbalance;
+  int64_t momentum_linear_iterations;
+  int64_t pressure_linear_iterations;
+  double device_ms;       /* whole solve, CUDA events on the context stream */
+  double pressure_solve_ms, momentum_solve_ms;
+  int64_t kernel_launches;
+} cfdb_simple_result;
+
+typedef struct cfdb_simple cfdb_simple;
+
+/* SIMPLE::solve (src/pressure_velocity/SIMPLE.cpp:148-1124), GPU-resident:
+ * every stage runs on the device and only scalars cross per outer iteration.
+ * u, v, w (ignored in 2D), p: host initial fields in, solution out; flux:
+ * host output (global face order); history (may be NULL): 5 doubles per
+ * outer iteration {u, v, w, p, continuity} residuals, up to max_outer rows. */
+CFDB_API cfdb_status cfdb_simple_solve(cfdb_context* ctx, const cfdb_simple_case* cs,
+                                       const cfdb_simple_settings* settings, double* u, double* v,
+                                       double* w, double* p, double* flux, double* history,
+                                       cfdb_simple_result* result);
+
+/* Stage-level session (the reference's GpuSimpleDiscretization,
+ * include/cfd/gpu/GpuSimpleDiscretization.hpp:56-262): upload a state, run
+ * single stages or outer iterations, read results back. */
+CFDB_API cfdb_status cfdb_simple_create(cfdb_context* ctx, const cfdb_simple_case* cs,
+                                        const cfdb_simple_settings* settings, cfdb_simple** out);
+CFDB_API void cfdb_simple_destroy(cfdb_simple* s);
+/* Uploads u, v, w, p and computes the face flux from u (calculateMassFlux). */
+CFDB_API cfdb_status cfdb_simple_set_state(cfdb_simple* s, const double* u, const double* v,
+                                           const double* w, const double* p);
+CFDB_API cfdb_status cfdb_simple_get_state(cfdb_simple* s, double* u, double* v, double* w,
+                                           double* p, double* flux);
+/* Green-Gauss gradient of p with the pressure BCs (Gradient.cpp:534-607). */
+CFDB_API cfdb_status cfdb_simple_pressure_gradient(cfdb_simple* s, double* gx, double* gy,
+                                                   double* gz);
+/* Relaxed momentum system of component comp from the current state
+ * (RelaxedMomentum.cpp:30-104): diag, off[6] (low/high neighbour per axis), rhs. */
+CFDB_API cfdb_status cfdb_simple_assemble_momentum(cfdb_simple* s, int comp, double* diag,
+                                                   double* const off[6], double* rhs);
+/* Runs up to n outer iterations from the current state (stops early on
+ * convergence or failure); history as in cfdb_simple_solve. */
+CFDB_API cfdb_status cfdb_simple_iterate(cfdb_simple* s, int64_t n, double* history,
+                                         cfdb_simple_result* result);
+
 #ifdef __cplusplus
 }
 #endif

@@ -910,6 +910,32 @@ static void assemble_momentum(const mctx* M, double* const U[3], int comp, const
   }
 }
 
+int og_momentum_system(const og_grid* g, const og_bcs* bc, const og_simple_settings* S, int comp,
+                       const double* u, const double* v, const double* w, const double* p,
+                       double* diag, double* const off[6], double* rhs) {
+  geo G;
+  geo_init(&G, g);
+  side_geo sg[3][2];
+  for (int a = 0; a < 3; ++a)
+    for (int s = 0; s < 2; ++s) sg[a][s] = (a < G.dim) ? side_geometry(&G, a, s) : (side_geo){0};
+  const int64_t n = G.nc;
+  double* mem = (double*)calloc((size_t)(13 * n + 2 * G.nf), sizeof(double));
+  if (!mem) return -1;
+  double* U[3] = {(double*)u, (double*)v, G.dim == 3 ? (double*)w : mem};
+  double* gradP[3] = {mem + n, mem + 2 * n, mem + 3 * n};
+  double* gradU[3] = {mem + 4 * n, mem + 5 * n, mem + 6 * n};
+  double* tmp[3] = {mem + 7 * n, mem + 8 * n, mem + 9 * n};
+  double* F = mem + 13 * n;
+  double* fv = F + G.nf;
+  mctx M = {&G, (const side_geo(*)[2])sg, bc, S->rho, S->mu, S->scheme};
+  mass_flux(&G, bc, S->rho, U, F);
+  gg_gradient(&G, sg, bc, p, fv, gradP, tmp);
+  velocity_gradient(&G, bc, U, comp, gradU);
+  assemble_momentum(&M, U, comp, F, gradP, gradU, S->alpha_u, diag, off, rhs);
+  free(mem);
+  return 0;
+}
+
 /* ------------------------------------------------------------ p' assembly */
 
 static int has_fixed_value(const geo* G, const og_bcs* bc) {

@@ -127,6 +127,13 @@ int og_simple(const og_grid* g, const og_bcs* bc, const og_simple_settings* s, d
               double* v, double* w, double* p, double* flux, double* hist,
               og_simple_result* out);
 
+/* The relaxed momentum system of component comp at the start of a SIMPLE
+ * solve from (u, v, w, p): flux from calculateMassFlux(U), then
+ * assembleRelaxedMomentumComponent (RelaxedMomentum.cpp:30-104). */
+int og_momentum_system(const og_grid* g, const og_bcs* bc, const og_simple_settings* s, int comp,
+                       const double* u, const double* v, const double* w, const double* p,
+                       double* diag, double* const off[6], double* rhs);
+
 /* Green-Gauss gradient of a scalar with pressure-type BCs (Gradient.cpp:534-607),
  * gx/gy/gz per cell. */
 int og_scalar_gradient(const og_grid* g, const og_bcs* bc, const double* phi, double* gx,

@@ -239,6 +239,22 @@ def scalar_gradient(case: Case, phi):
     return g[: case.dim]
 
 
+def momentum_system(case: Case, settings, comp: int, u, v, w, p):
+    """(diag, off[6], rhs) of the relaxed momentum system of `comp`."""
+    n = case.cells()
+    diag = np.zeros(n)
+    off = [np.zeros(n) for _ in range(6)]
+    rhs = np.zeros(n)
+    offp = (C.POINTER(C.c_double) * 6)(*[_dp(o) for o in off])
+    arr = [np.ascontiguousarray(a if a is not None else np.zeros(n), dtype=np.float64)
+           for a in (u, v, w, p)]
+    rc = lib().og_momentum_system(C.byref(case.c_grid()), C.byref(case.c_bcs()),
+                                  C.byref(settings.c(case.dim)), comp, *[_dp(a) for a in arr],
+                                  _dp(diag), offp, _dp(rhs))
+    assert rc == 0
+    return diag, off, rhs
+
+
 @dataclass
 class SimpleSettings:
     max_outer: int = 1000
