@@ -28,7 +28,9 @@ SIMPLE_STATUS = ["Converged", "MaxIterations", "MomentumFailure", "PressureCorre
 
 KRYLOV = {"cg": 0, "bicgstab": 1}
 PRECISION = {"fp64": 0, "fp32_refined": 1}
-PRECOND = {"none": 0, "jacobi": 1}
+PRECOND = {"none": 0, "jacobi": 1, "learned_mg": 2}
+MG_TAPS = 27
+MG_MAX_LEVELS = 16
 
 
 class CfdbError(RuntimeError):
@@ -51,7 +53,8 @@ class _LinResult(C.Structure):
                 ("true_residual", C.c_double), ("refinements", C.c_int64),
                 ("restarts", C.c_int64), ("device_ms", C.c_double),
                 ("kernel_launches", C.c_int64), ("krylov_ms", C.c_double),
-                ("krylov_bytes", C.c_double), ("krylov_launches", C.c_int64)]
+                ("krylov_bytes", C.c_double), ("krylov_launches", C.c_int64),
+                ("fallback_iterations", C.c_int64)]
 
 
 _lib = None
@@ -99,6 +102,11 @@ def load() -> C.CDLL:
     L.cfdb_copy_to_host.argtypes = [vp, vp, vp, C.c_size_t]
     L.cfdb_synchronize.argtypes = [vp]
     L.cfdb_memset_device.argtypes = [vp, vp, C.c_int, C.c_size_t]
+    fp = C.POINTER(C.c_float)
+    ip = C.POINTER(C.c_int)
+    L.cfdb_mg_set_weights.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, fp, fp]
+    L.cfdb_mg_get_weights.argtypes = [vp, C.c_int, ip, ip, ip, fp, fp]
+    L.cfdb_mg_reset_weights.argtypes = [vp, C.c_int, C.c_int]
     _lib = L
     return L
 
@@ -138,6 +146,35 @@ class Context:
 
     def launches(self) -> int:
         return int(self.lib.cfdb_kernel_launches(self._h))
+
+    # learned preconditioner weights (cfdb_mg_*)
+    def mg_set_weights(self, dim: int, kernels: np.ndarray, coarse_weights: np.ndarray,
+                       nu: int = 2, coarse_sweeps: int = 50):
+        """kernels: (levels, 27) float32 taps (x fastest); coarse_weights: (levels,)."""
+        k = np.ascontiguousarray(kernels, dtype=np.float32).reshape(-1, MG_TAPS)
+        c = np.ascontiguousarray(coarse_weights, dtype=np.float32).reshape(-1)
+        if len(c) != len(k):
+            raise ValueError("one coarse weight per kernel")
+        fp = C.POINTER(C.c_float)
+        self.check(self.lib.cfdb_mg_set_weights(self._h, dim, len(k), nu, coarse_sweeps,
+                                                k.ctypes.data_as(fp), c.ctypes.data_as(fp)),
+                   "cfdb_mg_set_weights")
+
+    def mg_get_weights(self, dim: int) -> dict:
+        lv, nu, cs = C.c_int(), C.c_int(), C.c_int()
+        k = np.zeros((MG_MAX_LEVELS, MG_TAPS), dtype=np.float32)
+        c = np.zeros(MG_MAX_LEVELS, dtype=np.float32)
+        fp = C.POINTER(C.c_float)
+        self.check(self.lib.cfdb_mg_get_weights(self._h, dim, C.byref(lv), C.byref(nu), C.byref(cs),
+                                                k.ctypes.data_as(fp), c.ctypes.data_as(fp)),
+                   "cfdb_mg_get_weights")
+        n = lv.value
+        return {"levels": n, "nu": nu.value, "coarse_sweeps": cs.value,
+                "kernels": k[:n].copy(), "coarse_weights": c[:n].copy()}
+
+    def mg_reset_weights(self, dim: int, trained: bool = True):
+        self.check(self.lib.cfdb_mg_reset_weights(self._h, dim, int(trained)),
+                   "cfdb_mg_reset_weights")
 
     def alloc(self, nbytes: int) -> int:
         p = C.c_void_p()
@@ -224,6 +261,7 @@ class SolverResult:
     krylov_ms: float
     krylov_bytes: float
     krylov_launches: int
+    fallback_iterations: int
     residual_history: np.ndarray
     solution: np.ndarray | None = None
 
@@ -288,11 +326,15 @@ class POperator:
             self.ctx.free(yd)
 
     def _result(self, r: _LinResult, hist, cap, sol=None) -> SolverResult:
-        m = min(cap, (r.iterations + 1) if self._precision == 0 else (r.refinements + 1))
+        if self._precond == PRECOND["learned_mg"]:
+            m = r.iterations - r.fallback_iterations + 1
+        else:
+            m = (r.iterations + 1) if self._precision == 0 else (r.refinements + 1)
+        m = min(cap, m)
         return SolverResult(SOLVER_STATUS[r.status], r.iterations, r.initial_residual,
                             r.final_residual, r.true_residual, r.refinements, r.restarts,
                             r.device_ms, r.kernel_launches, r.krylov_ms, r.krylov_bytes,
-                            r.krylov_launches, hist[:m].copy(), sol)
+                            r.krylov_launches, r.fallback_iterations, hist[:m].copy(), sol)
 
     def solve(self, b: np.ndarray, settings: LinearSolverSettings, x0: np.ndarray | None = None,
               history_cap: int | None = None) -> SolverResult:
@@ -304,6 +346,7 @@ class POperator:
         res = _LinResult()
         cs = settings.c()
         self._precision = cs.precision
+        self._precond = cs.preconditioner
         self.ctx.check(self.ctx.lib.cfdb_poperator_solve_host(self.ctx.handle, self._h, C.byref(cs),
                                                               _dp(b), _dp(x), _dp(hist), cap,
                                                               C.byref(res)), "cfdb_poperator_solve_host")
@@ -316,6 +359,7 @@ class POperator:
         res = _LinResult()
         cs = settings.c()
         self._precision = cs.precision
+        self._precond = cs.preconditioner
         self.ctx.check(self.ctx.lib.cfdb_poperator_solve_device(
             self.ctx.handle, self._h, C.byref(cs), C.c_void_p(b_dev), C.c_void_p(x_dev),
             _dp(hist) if history_cap > 0 else None, history_cap, C.byref(res)),

@@ -123,6 +123,7 @@ void cfdb_destroy(cfdb_context* ctx) {
   if (ctx->ev_k0) cudaEventDestroy(ctx->ev_k0);
   if (ctx->ev_k1) cudaEventDestroy(ctx->ev_k1);
   if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+  if (ctx->mg_weights_free) ctx->mg_weights_free(ctx->mg_weights);
   delete ctx;
 }
 

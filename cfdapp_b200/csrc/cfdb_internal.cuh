@@ -24,6 +24,9 @@ struct cfdb_context {
   double* scalars_host = nullptr;  // pinned mirror
   cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
   cudaEvent_t ev_k0 = nullptr, ev_k1 = nullptr;  // around persistent kernel launches
+  // Learned-preconditioner weights of this context (owned; see mg.cu).
+  void* mg_weights = nullptr;
+  void (*mg_weights_free)(void*) = nullptr;
 };
 
 namespace cfdb {

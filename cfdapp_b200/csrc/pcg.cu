@@ -28,6 +28,7 @@
 #include "cfdb.h"
 #include "cfdb_internal.cuh"
 #include "grid_sync.cuh"
+#include "mg.cuh"
 #include "poperator.cuh"
 #include "tile.cuh"
 #include "tma.cuh"
@@ -52,6 +53,8 @@ struct cfdb_poperator {
   double* invd64 = nullptr;  // 1/diag, face-coefficient operators only
   float* invd32 = nullptr;
   bool faces_borrowed = false;  // f64[] point into a caller's device array
+  uint64_t version = 1;         // bumped whenever the coefficients change
+  cfdb::LearnedSolver* learned = nullptr;
 };
 
 namespace cfdb {
@@ -731,6 +734,72 @@ cfdb_status solve_refined(cfdb_context* ctx, cfdb_poperator* op, const cfdb_line
   return CFDB_OK;
 }
 
+// Learned V-cycle inside FP64 flexible CG; when it stagnates (or breaks
+// down) the FP64 Jacobi-PCG continues from its iterate with the remaining
+// iteration budget and the original tolerance.
+cfdb_status solve_learned(cfdb_context* ctx, cfdb_poperator* op, const cfdb_linear_settings* s,
+                          const double* b, double* x, double* history, int64_t history_cap,
+                          cfdb_linear_result* res) {
+  const cfdb_grid& g = op->grid;
+  FineOperator fo;
+  std::memset(&fo, 0, sizeof(fo));
+  fo.dim = g.dim;
+  fo.n[0] = (int)g.n[0];
+  fo.n[1] = (int)g.n[1];
+  fo.n[2] = g.dim == 3 ? (int)g.n[2] : 1;
+  fo.A = view<double>(op);
+  const int kaxis[3] = {0, g.dim == 2 ? 2 : 1, 2};
+  for (int a = 0; a < g.dim; ++a) {
+    fo.full[a] = op->f64[kaxis[a]];
+    fo.table[a] = op->t64[kaxis[a]];
+  }
+  fo.pinned = op->pinned;
+  fo.ref = op->ref;
+  if (!op->learned) op->learned = learned_create();
+  const int64_t cap = std::min<int64_t>(s->max_iterations, 100000);
+  LearnedOutcome o;
+  cfdb_status st = learned_solve(ctx, op->learned, fo, op->version, mg_context_weights(ctx, g.dim),
+                                 b, x, s->abs_tol, s->rel_tol, cap,
+                                 std::max<int64_t>(history_cap, 1), &o);
+  if (st != CFDB_OK) return st;
+  res->initial_residual = o.initial_residual;
+  res->final_residual = o.final_residual;
+  res->iterations = o.iterations;
+  res->status = o.status;
+  res->krylov_ms += o.kernel_ms;
+  res->krylov_bytes += o.bytes;
+  res->krylov_launches += 1;
+  if (history && history_cap > 0) {
+    st = learned_history(ctx, op->learned, history, std::min<int64_t>(history_cap, o.iterations + 1));
+    if (st != CFDB_OK) return st;
+  }
+  const bool stalled = o.status == kLearnedStagnated ||
+                       (o.status == CFDB_SOLVER_MAX_ITERATIONS && cap < s->max_iterations);
+  if (!stalled) return CFDB_OK;
+  const int64_t left = s->max_iterations - o.iterations;
+  if (left < 1) {
+    res->status = CFDB_SOLVER_MAX_ITERATIONS;
+    return CFDB_OK;
+  }
+  cfdb_linear_settings s2 = *s;
+  s2.max_iterations = left;
+  // keep the caller's relative target, measured against the original start
+  if (o.final_residual > 0.0 && std::isfinite(o.final_residual))
+    s2.rel_tol = s->rel_tol * o.initial_residual / o.final_residual;
+  cfdb_linear_result sub;
+  std::memset(&sub, 0, sizeof(sub));
+  st = solve_fp64(ctx, op, &s2, b, x, false, 0, &sub);
+  if (st != CFDB_OK) return st;
+  res->status = sub.status;
+  res->iterations += sub.iterations;
+  res->fallback_iterations = sub.iterations;
+  res->final_residual = sub.final_residual;
+  res->krylov_ms += sub.krylov_ms;
+  res->krylov_bytes += sub.krylov_bytes;
+  res->krylov_launches += sub.krylov_launches;
+  return CFDB_OK;
+}
+
 cfdb_status build_tables(cfdb_context* ctx, cfdb_poperator* op, double rho, unsigned dmask) {
   // Geometry exactly as the reference evaluates it (MeshGrading.cpp
   // AxisSpacing::uniform/center/node; MeshGeometry.cpp:513-552,1047-1140):
@@ -844,6 +913,7 @@ cfdb_status poperator_bind_faces(cfdb_context* ctx, cfdb_poperator* op, const do
   const int64_t offs[3] = {0, nfx, nfx + nfy};
   const int kaxis[3] = {0, g.dim == 2 ? 2 : 1, 2};
   op->faces_borrowed = true;
+  ++op->version;
   for (int a = 0; a < g.dim; ++a) {
     const int ka = kaxis[a];
     op->f64[ka] = const_cast<double*>(D + offs[a]);
@@ -951,6 +1021,7 @@ void cfdb_poperator_destroy(cfdb_poperator* op) {
   cudaFree(op->hist_dev);
   cudaFree(op->invd64);
   cudaFree(op->invd32);
+  cfdb::learned_destroy(op->learned);
   delete op;
 }
 
@@ -983,8 +1054,9 @@ cfdb_status cfdb_poperator_solve_device(cfdb_context* ctx, const cfdb_poperator*
   std::memset(result, 0, sizeof(*result));
   if (s->krylov != CFDB_KRYLOV_CG)
     return set_error(ctx, CFDB_ERR_UNSUPPORTED, "the structured p' solve runs CG");
-  if (s->preconditioner != CFDB_PRECOND_JACOBI)
-    return set_error(ctx, CFDB_ERR_UNSUPPORTED, "the structured p' solve is Jacobi-preconditioned");
+  if (s->preconditioner != CFDB_PRECOND_JACOBI && s->preconditioner != CFDB_PRECOND_LEARNED_MG)
+    return set_error(ctx, CFDB_ERR_UNSUPPORTED,
+                     "the structured p' solve takes the Jacobi or the learned preconditioner");
   if (s->max_iterations < 1)
     return set_error(ctx, CFDB_ERR_INVALID_ARGUMENT, "max_iterations must be >= 1");
   if (history_cap < 0) history_cap = 0;
@@ -1001,7 +1073,9 @@ cfdb_status cfdb_poperator_solve_device(cfdb_context* ctx, const cfdb_poperator*
     return CFDB_OK;
   }
   CFDB_CUDA(ctx, cudaEventRecord(ctx->ev_start, ctx->stream));
-  if (s->precision == CFDB_PRECISION_FP32_REFINED) {
+  if (s->preconditioner == CFDB_PRECOND_LEARNED_MG) {
+    st = solve_learned(ctx, op, s, b_dev, x_dev, history, history_cap, result);
+  } else if (s->precision == CFDB_PRECISION_FP32_REFINED) {
     st = solve_refined(ctx, op, s, b_dev, x_dev, history_cap, history, result);
   } else {
     st = solve_fp64(ctx, op, s, b_dev, x_dev, false, history_cap, result);

@@ -330,7 +330,8 @@ cfdb_status outer_iteration(cfdb_simple* s, int64_t it, double* hist, cfdb_simpl
   CFDB_CUDA(ctx, cudaMemsetAsync(s->pp, 0, sizeof(double) * s->n, st));
   cfdb_linear_result pr;
   const bool use_pcg = S.pressure.krylov == CFDB_KRYLOV_CG &&
-                       S.pressure.preconditioner == CFDB_PRECOND_JACOBI;
+                       (S.pressure.preconditioner == CFDB_PRECOND_JACOBI ||
+                        S.pressure.preconditioner == CFDB_PRECOND_LEARNED_MG);
   if (use_pcg) {
     rc = poperator_bind_faces(ctx, s->pop, s->D, S.pressure.precision == CFDB_PRECISION_FP32_REFINED);
     if (rc != CFDB_OK) return rc;

@@ -77,7 +77,12 @@ enum {
   CFDB_PRECISION_FP64 = 0,          /* every sweep in FP64 (the reference's arithmetic) */
   CFDB_PRECISION_FP32_REFINED = 1   /* FP32 inner sweeps inside FP64 iterative refinement */
 };
-enum { CFDB_PRECOND_NONE = 0, CFDB_PRECOND_JACOBI = 1 };
+enum {
+  CFDB_PRECOND_NONE = 0,
+  CFDB_PRECOND_JACOBI = 1,     /* JacobiPreconditioner (src/algebra/Preconditioner.cpp:11-49) */
+  CFDB_PRECOND_LEARNED_MG = 2  /* no counterpart in the reference: learned V-cycle inside FP64
+                                  flexible CG; Jacobi-PCG takes over if it stagnates */
+};
 
 /* LinearSolverSettings (LinearSolver.hpp:136-166) plus the precision knobs. */
 typedef struct {
@@ -105,6 +110,7 @@ typedef struct {
   double krylov_ms;           /* device time inside the persistent Krylov kernels */
   double krylov_bytes;        /* algorithmic bytes those kernels move (words read + written) */
   int64_t krylov_launches;    /* number of persistent Krylov kernel launches */
+  int64_t fallback_iterations;/* LEARNED_MG: Jacobi-PCG iterations after a stagnated learned solve */
 } cfdb_linear_result;
 
 /* ------------------------------------------------------------------ context */
@@ -269,6 +275,26 @@ CFDB_API cfdb_status cfdb_simple_assemble_momentum(cfdb_simple* s, int comp, dou
  * convergence or failure); history as in cfdb_simple_solve. */
 CFDB_API cfdb_status cfdb_simple_iterate(cfdb_simple* s, int64_t n, double* history,
                                          cfdb_simple_result* result);
+
+/* ------------------------------------------- learned preconditioner weights */
+
+/* No counterpart in the reference.  Weights of the CFDB_PRECOND_LEARNED_MG
+ * V-cycle used by this context's solves of dimension `dim` (2 or 3):
+ * `levels` kernels of 27 taps each (3x3x3, x fastest; 2D kernels use taps
+ * 9..17 only and must leave the others 0), point-symmetric (tap t equals tap
+ * 26-t), one coarse-correction weight per level; levels deeper than `levels`
+ * reuse the last kernel.  nu = smoothing sweeps per side (1..8),
+ * coarse_sweeps = damped-Jacobi sweeps on the coarsest level (0..1000).
+ * Invalid sets return CFDB_ERR_INVALID_ARGUMENT and change nothing. */
+CFDB_API cfdb_status cfdb_mg_set_weights(cfdb_context* ctx, int dim, int levels, int nu,
+                                         int coarse_sweeps, const float* kernels,
+                                         const float* coarse_weights);
+/* Reads the current set: kernels[16*27], coarse_weights[16] (any may be NULL). */
+CFDB_API cfdb_status cfdb_mg_get_weights(cfdb_context* ctx, int dim, int* levels, int* nu,
+                                         int* coarse_sweeps, float* kernels,
+                                         float* coarse_weights);
+/* trained = 1: the weights shipped with the library; 0: untrained damped Jacobi. */
+CFDB_API cfdb_status cfdb_mg_reset_weights(cfdb_context* ctx, int dim, int trained);
 
 /* ------------------------------------------------------ allocation-free solve */
 

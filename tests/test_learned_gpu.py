@@ -1,0 +1,153 @@
+"""The learned-preconditioner p' solve (CFDB_PRECOND_LEARNED_MG): a V-cycle
+network inside FP64 flexible CG, falling back to Jacobi-PCG on stagnation.
+
+It has no counterpart in the reference, so the bars are the reference's own
+acceptance quantities: the same converged status and the same FP64
+relative-residual target as CG + Jacobi (src/algebra/CG.cpp:14-148), the
+true residual recomputed on the CPU by the oracle from the returned x, and a
+solution within 1e-7 relative L2 of the oracle's CG solution when both are
+driven to 1e-11.  The point of the method -- far fewer iterations than
+Jacobi-PCG -- is asserted too.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _settings(**kw):
+    from cfdapp_b200.cfdb import LinearSolverSettings
+    base = dict(absolute_tolerance=0.0, relative_tolerance=1e-8, max_iterations=100000,
+                preconditioner="learned_mg")
+    base.update(kw)
+    return LinearSolverSettings(**base)
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def _true_rel_residual(case, diag, off, b, x):
+    return float(np.linalg.norm(b - O.stencil_apply(case, diag, off, x)) / np.linalg.norm(b))
+
+
+@pytest.mark.parametrize("dim,n", [(2, 64), (2, 256), (3, 16), (3, 48)])
+def test_learned_reaches_tolerance_in_few_iterations(ctx, dim, n):
+    from cfdapp_b200.cfdb import POperator
+    case, fc, diag, off, b = O.isolated_pprime(dim, n)
+    op = POperator(ctx, dim, [n] * dim)
+    res = op.solve(b, _settings())
+    jac = op.solve(b, _settings(preconditioner="jacobi"))
+    assert res.status == jac.status == "Converged"
+    assert res.fallback_iterations == 0
+    assert _true_rel_residual(case, diag, off, b, res.solution) <= 1.05e-8
+    assert res.true_residual / res.initial_residual <= 1.05e-8
+    assert res.residual_history[0] == pytest.approx(res.initial_residual)
+    assert res.residual_history[-1] / res.initial_residual <= 1e-8
+    assert res.iterations * 4 <= jac.iterations
+
+
+@pytest.mark.parametrize("dim,n", [(2, 128), (3, 24)])
+def test_learned_solution_matches_oracle(ctx, dim, n):
+    from cfdapp_b200.cfdb import POperator
+    case, fc, diag, off, b = O.isolated_pprime(dim, n)
+    ref = O.stencil_solve(case, diag, off, b, rel_tol=1e-11, history=False)
+    op = POperator(ctx, dim, [n] * dim)
+    res = op.solve(b, _settings(relative_tolerance=1e-11))
+    assert res.status == ref.status == "Converged"
+    assert _rel(res.solution, ref.solution) <= 1e-7
+
+
+def test_learned_face_operator_non_square(ctx):
+    """Per-face coefficients of a SIMPLE iteration (random response field)."""
+    from cfdapp_b200.cfdb import POperator
+    case = O.Case(2, (96, 80), (1.2, 1.0), [("wall", (0, 0, 0))] * 4,
+                  [("fixed_gradient", 0.0)] * 4)
+    rng = np.random.default_rng(11)
+    cells = case.cells()
+    du = np.exp(rng.normal(size=cells) * 0.5)
+    dv = np.exp(rng.normal(size=cells) * 0.5)
+    flux = rng.normal(size=case.faces()) * 1e-3
+    fc, diag, off, rhs = O.assemble_pprime(case, 1.0, flux, du, dv)
+    op = POperator(ctx, 2, (96, 80), (1.2, 1.0), face_coeff=fc)
+    res = op.solve(rhs, _settings())
+    assert res.status == "Converged"
+    assert _true_rel_residual(case, diag, off, rhs, res.solution) <= 1.05e-8
+    ref = O.stencil_solve(case, diag, off, rhs, history=False)
+    assert res.iterations * 3 <= ref.iterations
+
+
+def test_learned_dirichlet_unpinned(ctx):
+    from cfdapp_b200.cfdb import POperator
+    case = O.channel(64, 16, 4.0, 1.0)
+    ones = np.ones(case.cells())
+    rng = np.random.default_rng(3)
+    flux = rng.normal(size=case.faces()) * 1e-2
+    fc, diag, off, rhs = O.assemble_pprime(case, 1.0, flux, ones, ones)
+    op = POperator(ctx, 2, (64, 16), (4.0, 1.0), face_coeff=fc, pinned=False)
+    res = op.solve(rhs, _settings())
+    assert res.status == "Converged"
+    assert _true_rel_residual(case, diag, off, rhs, res.solution) <= 1.05e-8
+
+
+def test_learned_status_edge_cases(ctx):
+    from cfdapp_b200.cfdb import POperator
+    op = POperator(ctx, 2, (32, 32))
+    zero = op.solve(np.zeros(1024), _settings())
+    assert zero.status == "Converged" and zero.iterations == 0
+    b = O.synth_rhs(2, 32)
+    capped = op.solve(b, _settings(max_iterations=3))
+    assert capped.status == "MaxIterations" and capped.iterations == 3
+    bad = b.copy()
+    bad[5] = np.inf
+    assert op.solve(bad, _settings()).status == "NonFiniteInput"
+    loose = op.solve(b, _settings(absolute_tolerance=1.0))
+    assert loose.status == "Converged" and loose.iterations == 0
+    # repeated solves reuse the captured graph and give identical results
+    r1 = op.solve(b, _settings())
+    r2 = op.solve(b, _settings())
+    assert r1.iterations == r2.iterations
+    np.testing.assert_array_equal(r1.solution, r2.solution)
+
+
+def test_learned_falls_back_to_jacobi_when_the_network_is_useless(ctx):
+    """A zero network gives z = 0: FCG stops and Jacobi-PCG finishes the solve."""
+    from cfdapp_b200.cfdb import POperator
+    case, fc, diag, off, b = O.isolated_pprime(2, 48)
+    op = POperator(ctx, 2, (48, 48))
+    try:
+        ctx.mg_set_weights(2, np.zeros((1, 27), np.float32), np.zeros(1, np.float32),
+                           coarse_sweeps=0)
+        res = op.solve(b, _settings())
+    finally:
+        ctx.mg_reset_weights(2, trained=True)
+    assert res.status == "Converged"
+    assert res.fallback_iterations > 0
+    assert _true_rel_residual(case, diag, off, b, res.solution) <= 1.05e-8
+
+
+def test_weights_api(ctx):
+    from cfdapp_b200.cfdb import CfdbError
+    w = ctx.mg_get_weights(3)
+    assert w["kernels"].shape == (w["levels"], 27)
+    bad = np.zeros((1, 27), np.float32)
+    bad[0, 12] = 1.0  # not point-symmetric
+    with pytest.raises(CfdbError):
+        ctx.mg_set_weights(3, bad, np.ones(1, np.float32))
+    flat = np.zeros((1, 27), np.float32)
+    flat[0, 0] = 1.0  # 2D kernels live in the middle plane only
+    flat[0, 26] = 1.0
+    with pytest.raises(CfdbError):
+        ctx.mg_set_weights(2, flat, np.ones(1, np.float32))
+    k = np.zeros((2, 27), np.float32)
+    k[:, 13] = 0.7
+    k[:, 12] = k[:, 14] = 0.05
+    ctx.mg_set_weights(3, k, np.array([1.0, 0.9], np.float32), nu=3, coarse_sweeps=20)
+    got = ctx.mg_get_weights(3)
+    assert got["levels"] == 2 and got["nu"] == 3 and got["coarse_sweeps"] == 20
+    np.testing.assert_array_equal(got["kernels"], k)
+    ctx.mg_reset_weights(3, trained=False)
+    assert ctx.mg_get_weights(3)["kernels"][0, 13] == np.float32(0.8)
+    ctx.mg_reset_weights(3, trained=True)
