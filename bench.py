@@ -7,8 +7,10 @@ Workload: the reference's p' operator for unit response coefficients
 random-phase sinusoids), solved from x0 = 0 to an FP64-verified relative
 residual of 1e-8.  One step = one solve of the 2048^2 system plus one of the
 256^3 system.  `value` is the device time per step of the headline solver
-(FP32-inner / FP64-refined PCG), inputs resident in HBM; the plain FP64
-Jacobi-PCG of the same library is timed beside it (`fp64_jacobi_pcg_ms`).
+(FP64 flexible CG preconditioned by the learned FP32 V-cycle, looped on the
+device by one CUDA graph), inputs resident in HBM; the plain FP64 Jacobi-PCG
+of the same library (the reference's method) is timed beside it
+(`fp64_jacobi_pcg_ms`), and the FP32-inner / FP64-refined Jacobi-PCG too.
 `e2e` times the same step through the C ABI with host buffers (copies in the
 timed region).  Multi-GPU runs are independent replicas (the solve does not
 shard); `value` is then the max over ranks of the per-step time.
@@ -246,6 +248,8 @@ def main():
                                     max_iterations=200000, precision="fp64")
     s32 = cfdb.LinearSolverSettings(absolute_tolerance=0.0, relative_tolerance=1e-8,
                                     max_iterations=400000, precision="fp32_refined")
+    smg = cfdb.LinearSolverSettings(absolute_tolerance=0.0, relative_tolerance=1e-8,
+                                    max_iterations=200000, preconditioner="learned_mg")
     systems = []
     for dim, n in grids:
         b = cfdb.synth_rhs(dim, n, SEED)
@@ -275,11 +279,18 @@ def main():
             assert r.status == "Converged", r
             ms.append(r.device_ms)
         fp64[(s[0], s[1])] = (statistics.mean(ms), r)
+    # ---- FP32-inner Jacobi-PCG in FP64 refinement (one timed solve each)
+    fp32r = {}
+    for s in systems:
+        solve(s, s32)
+        l2_flush()
+        r = solve(s, s32)
+        fp32r[(s[0], s[1])] = r
 
     # ---- headline solver: warm-up
     for _ in range(a.warmup):
         for s in systems:
-            solve(s, s32)
+            solve(s, smg)
     if torch_dist:
         torch_dist.barrier()
     ctx.synchronize()
@@ -292,7 +303,7 @@ def main():
         tot = 0.0
         for s in systems:
             l2_flush()
-            r = solve(s, s32)
+            r = solve(s, smg)
             if r.status != "Converged" or r.true_residual / r.initial_residual > 1e-8:
                 raise SystemExit(f"bench: solve did not reach 1e-8: {r}")
             tot += r.device_ms
@@ -317,7 +328,7 @@ def main():
         for dim, n, b, op, bd, xd in systems:
             x = np.zeros(b.size)
             t0 = time.perf_counter()
-            r = op.solve(b, s32, x0=x, history_cap=0)
+            r = op.solve(b, smg, x0=x, history_cap=0)
             tot += (time.perf_counter() - t0) * 1e3
             assert r.status == "Converged"
         e2e.append(tot)
@@ -326,7 +337,7 @@ def main():
         d2h += b.nbytes       # x
     e2e_ms = statistics.mean(e2e)
 
-    # ---- roofline of the dominant kernel (the persistent FP32 PCG)
+    # ---- roofline of the solve graph (V-cycle + FCG kernels, one launch)
     peak, peak_kind = measured_peaks()
     kms = sum(r.krylov_ms for rs in per_grid.values() for r in rs)
     kbytes = sum(r.krylov_bytes for rs in per_grid.values() for r in rs)
@@ -336,7 +347,7 @@ def main():
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
         try:
-            traffic = json.load(open(tpath)).get("pcg_persistent_fp32_bytes_per_launch")
+            traffic = json.load(open(tpath)).get("learned_fcg_bytes_per_launch")
         except ValueError:
             traffic = None
 
@@ -348,8 +359,10 @@ def main():
             "headline_ms": mean_ms, "fp64_jacobi_pcg_ms": f64ms,
             "speedup_vs_fp64_jacobi_pcg": f64ms / mean_ms,
             "fp64_iterations": f64r.iterations,
-            "inner_iterations": rs[-1].iterations, "refinements": rs[-1].refinements,
+            "iterations": rs[-1].iterations, "fallback_iterations": rs[-1].fallback_iterations,
             "true_rel_residual": rs[-1].true_residual / rs[-1].initial_residual,
+            "solve_graph_gbs": rs[-1].krylov_bytes / (rs[-1].krylov_ms * 1e-3) / 1e9,
+            "fp32_refined_jacobi_pcg_ms": fp32r[(dim, n)].device_ms,
             "fp64_true_rel_residual": f64r.true_residual / f64r.initial_residual,
             "fp64_pcg_gbs": f64r.krylov_bytes / (f64r.krylov_ms * 1e-3) / 1e9,
         }
@@ -361,12 +374,13 @@ def main():
         line = {
             "metric": METRIC, "value": ms_step, "unit": "ms", "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms_step, "higher_is_better": False,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32 inner / f64 refined",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64 (FCG) / f32 (V-cycle)",
             "data": "synthetic",
             "config": {"workload": "isolated p' solve: 5-point 2048^2 + 7-point 256^3, "
                                    "Neumann + pinned cell, seeded 32-sinusoid RHS, x0=0, "
                                    "rel-res 1e-8 (FP64-verified)",
-                       "solver": "FP32-inner Jacobi-PCG in FP64 iterative refinement",
+                       "solver": "FP64 flexible CG + learned FP32 V-cycle preconditioner "
+                                 "(CUDA graph WHILE loop)",
                        "grids": [f"{d}D {n}" for d, n in grids],
                        "l2": "flushed (512 MiB write) before every timed solve",
                        "parallelism": f"replicas x{world}"},
@@ -375,7 +389,7 @@ def main():
             "grids": grid_detail,
             "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
-            "roofline": {"bound": "hbm", "kernel": "pcg_persistent<float>",
+            "roofline": {"bound": "hbm", "kernel": "learned-FCG solve graph (all its kernels)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None,
                          "peak_source": f"{peak_kind} hbm_gbs",

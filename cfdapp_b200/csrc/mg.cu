@@ -18,6 +18,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 
@@ -223,18 +224,30 @@ __device__ __forceinline__ void reduce_last(double (&v)[NV], double* partials, u
   }
 }
 
+
+// The WHILE node's condition, or nothing when the kernels run outside a
+// graph (stream mode: active = 0).
+struct Loop {
+  cudaGraphConditionalHandle h;
+  int active;
+};
+
+__device__ __forceinline__ void set_loop(const Loop& lp, unsigned v) {
+  if (lp.active) cudaGraphSetConditional(lp.h, v);
+}
+
+__device__ __forceinline__ void stop_loop(FcgState* S, const Loop& h, int status) {
+  S->status = status;
+  S->done = 1;
+  set_loop(h, 0);
+}
+
 struct Hook {
   const double* q;  // previous A p
   double* partials;
   FcgState* S;
-  cudaGraphConditionalHandle h;
+  Loop h;
 };
-
-__device__ __forceinline__ void stop_loop(FcgState* S, cudaGraphConditionalHandle h, int status) {
-  S->status = status;
-  S->done = 1;
-  cudaGraphSetConditional(h, 0);
-}
 
 // ------------------------------------------------------------ level kernels
 
@@ -670,7 +683,7 @@ double cycle_bytes(const MgHierarchy& H, const MgWeights& W) {
 // r = b - A x, r32 = float(r); ||r|| decides whether the loop runs at all.
 __global__ void k_fcg_init(OpView<double> A, FcgState* S, double* __restrict__ r,
                            float* __restrict__ r32, double* partials, double* hist, int64_t hcap,
-                           cudaGraphConditionalHandle h) {
+                           Loop h) {
   const double* __restrict__ b = S->b;
   const double* __restrict__ x = S->x;
   double acc[1] = {0.0};
@@ -702,7 +715,7 @@ __global__ void k_fcg_init(OpView<double> A, FcgState* S, double* __restrict__ r
     } else {
       S->status = kRunning;
       S->done = 0;
-      cudaGraphSetConditional(h, 1);
+      set_loop(h, 1);
     }
   });
 }
@@ -712,7 +725,7 @@ __global__ void k_fcg_init(OpView<double> A, FcgState* S, double* __restrict__ r
 __global__ void k_fcg_dir(OpView<double> A, FcgState* S, const float* __restrict__ z,
                           double* P0, double* P1, double* __restrict__ q,
                           const double* __restrict__ r, double* partials,
-                          cudaGraphConditionalHandle h) {
+                          Loop h) {
   if (S->done) return;
   const long long it = S->it;
   const bool first = (it == 0);
@@ -737,7 +750,10 @@ __global__ void k_fcg_dir(OpView<double> A, FcgState* S, const float* __restrict
   reduce_last<2>(acc, partials, &S->ticket, [&](const double* tot) {
     const double pq = tot[0], pr = tot[1];
     const double alpha = pr / pq;
-    if (!isfinite(pq) || fabs(pq) < 1.0e-30 || !isfinite(alpha)) {
+    // A is positive definite on the space the directions live in: a
+    // non-positive p.Ap means rounding has taken over (a scale-free test; the
+    // reference's absolute 1e-30 trips on small well-converged systems)
+    if (!isfinite(pq) || !(pq > 0.0) || !isfinite(alpha)) {
       stop_loop(S, h, kLearnedStagnated);
       return;
     }
@@ -752,7 +768,7 @@ __global__ void k_fcg_dir(OpView<double> A, FcgState* S, const float* __restrict
 __global__ void k_fcg_update(int64_t n, FcgState* S, double* __restrict__ r,
                              float* __restrict__ r32, const double* P0, const double* P1,
                              const double* __restrict__ q, double* partials, double* hist,
-                             int64_t hcap, cudaGraphConditionalHandle h) {
+                             int64_t hcap, Loop h) {
   if (S->done) return;
   const long long it = S->it;
   const double alpha = S->alpha;
@@ -924,9 +940,42 @@ int64_t partial_slots(const FineOperator& op) {
   return std::max<int64_t>((int64_t)sh.grid.x * sh.grid.y, kMaxBlocks);
 }
 
+// One FCG iteration: V-cycle z = M r (its last kernel also forms z.q and
+// beta), direction + A p, update.  Returns the number of kernels.
+int enqueue_body(LearnedSolver* s, const FineOperator& op, Loop h, cudaStream_t st) {
+  const int64_t skip = op.pinned ? op.ref : -1;
+  const Shape sh = cells_shape(op.A.nx, (int64_t)op.A.ny * op.A.nz);
+  const Hook hk{s->q, s->partials, s->S, h};
+  const int nv = op.dim == 2 ? enqueue_cycle<2>(*s->H, s->W, s->r32, s->z32, skip, &hk, st)
+                             : enqueue_cycle<3>(*s->H, s->W, s->r32, s->z32, skip, &hk, st);
+  k_fcg_dir<<<sh.grid, sh.block, 0, st>>>(op.A, s->S, s->z32, s->p0, s->p1, s->q, s->r,
+                                           s->partials, h);
+  k_fcg_update<<<flat_grid(s->cells), 256, 0, st>>>(s->cells, s->S, s->r, s->r32, s->p0, s->p1,
+                                                    s->q, s->partials, s->hist, s->hist_cap, h);
+  return nv + 2;
+}
+
+// Solve loop without a graph, for profilers that cannot look inside graphs
+// with conditional nodes (CFDB_LEARNED_LAUNCH=stream): the same kernels,
+// launched per iteration, the host reading the state after each iteration.
+cfdb_status run_stream_mode(cfdb_context* ctx, LearnedSolver* s, const FineOperator& op) {
+  const Shape sh = cells_shape(op.A.nx, (int64_t)op.A.ny * op.A.nz);
+  k_fcg_init<<<sh.grid, sh.block, 0, ctx->stream>>>(op.A, s->S, s->r, s->r32, s->partials, s->hist,
+                                                     s->hist_cap, Loop{0, 0});
+  CFDB_CHECK_LAUNCH(ctx);
+  while (true) {
+    CFDB_CUDA(ctx, cudaMemcpyAsync(s->S_host, s->S, sizeof(FcgState), cudaMemcpyDeviceToHost,
+                                   ctx->stream));
+    CFDB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (s->S_host->done) break;
+    enqueue_body(s, op, Loop{0, 0}, ctx->stream);
+    CFDB_CHECK_LAUNCH(ctx);
+  }
+  return CFDB_OK;
+}
+
 cfdb_status capture_graph(cfdb_context* ctx, LearnedSolver* s, const FineOperator& op) {
   s->free_graph();
-  const int64_t skip = op.pinned ? op.ref : -1;
   CFDB_CUDA(ctx, cudaGraphCreate(&s->graph, 0));
   cudaGraphConditionalHandle h;
   CFDB_CUDA(ctx, cudaGraphConditionalHandleCreate(&h, s->graph, 1, cudaGraphCondAssignDefault));
@@ -934,8 +983,9 @@ cfdb_status capture_graph(cfdb_context* ctx, LearnedSolver* s, const FineOperato
   // parent graph: the initial residual, then the WHILE node
   CFDB_CUDA(ctx, cudaStreamBeginCaptureToGraph(s->cap, s->graph, nullptr, nullptr, 0,
                                                cudaStreamCaptureModeThreadLocal));
+  const Loop lp{h, 1};
   k_fcg_init<<<sh.grid, sh.block, 0, s->cap>>>(op.A, s->S, s->r, s->r32, s->partials, s->hist,
-                                                s->hist_cap, h);
+                                                s->hist_cap, lp);
   cudaGraph_t g = nullptr;
   cudaError_t ce = cudaStreamEndCapture(s->cap, &g);
   if (ce != cudaSuccess) return cuda_error(ctx, ce, "capture of the FCG start", __FILE__, __LINE__);
@@ -954,20 +1004,14 @@ cfdb_status capture_graph(cfdb_context* ctx, LearnedSolver* s, const FineOperato
   // body: one FCG iteration
   CFDB_CUDA(ctx, cudaStreamBeginCaptureToGraph(s->cap, body, nullptr, nullptr, 0,
                                                cudaStreamCaptureModeThreadLocal));
-  const Hook hk{s->q, s->partials, s->S, h};
-  const int nv = op.dim == 2 ? enqueue_cycle<2>(*s->H, s->W, s->r32, s->z32, skip, &hk, s->cap)
-                             : enqueue_cycle<3>(*s->H, s->W, s->r32, s->z32, skip, &hk, s->cap);
-  k_fcg_dir<<<sh.grid, sh.block, 0, s->cap>>>(op.A, s->S, s->z32, s->p0, s->p1, s->q, s->r,
-                                               s->partials, h);
-  k_fcg_update<<<flat_grid(s->cells), 256, 0, s->cap>>>(s->cells, s->S, s->r, s->r32, s->p0, s->p1,
-                                                        s->q, s->partials, s->hist, s->hist_cap, h);
+  const int nv = enqueue_body(s, op, lp, s->cap);
   cudaGraph_t b2 = nullptr;
   ce = cudaStreamEndCapture(s->cap, &b2);
   if (ce != cudaSuccess) return cuda_error(ctx, ce, "capture of the FCG loop", __FILE__, __LINE__);
   CFDB_CHECK_LAUNCH(ctx);
   CFDB_CUDA(ctx, cudaGraphInstantiate(&s->exec, s->graph, 0));
   s->launches_init = 1;
-  s->launches_body = nv + 2;
+  s->launches_body = nv;
   // algorithmic bytes: the start (b, x in; r, r32 out) and per iteration the
   // V-cycle, the direction pass (z, p_old, r in; p, q out), the update (x, p,
   // r, q in; x, r, r32 out) and the z.q read of q; face arrays when present
@@ -1061,7 +1105,13 @@ cfdb_status learned_solve(cfdb_context* ctx, LearnedSolver* s, const FineOperato
   hs.status = kRunning;
   CFDB_CUDA(ctx, cudaMemcpyAsync(s->S, &hs, sizeof(FcgState), cudaMemcpyHostToDevice, ctx->stream));
   CFDB_CUDA(ctx, cudaEventRecord(ctx->ev_k0, ctx->stream));
-  CFDB_CUDA(ctx, cudaGraphLaunch(s->exec, ctx->stream));
+  const char* mode = std::getenv("CFDB_LEARNED_LAUNCH");
+  if (mode && std::strcmp(mode, "stream") == 0) {
+    cfdb_status st = run_stream_mode(ctx, s, op);
+    if (st != CFDB_OK) return st;
+  } else {
+    CFDB_CUDA(ctx, cudaGraphLaunch(s->exec, ctx->stream));
+  }
   CFDB_CUDA(ctx, cudaEventRecord(ctx->ev_k1, ctx->stream));
   CFDB_CUDA(ctx, cudaMemcpyAsync(s->S_host, s->S, sizeof(FcgState), cudaMemcpyDeviceToHost, ctx->stream));
   CFDB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));

@@ -5,8 +5,9 @@ It has no counterpart in the reference, so the bars are the reference's own
 acceptance quantities: the same converged status and the same FP64
 relative-residual target as CG + Jacobi (src/algebra/CG.cpp:14-148), the
 true residual recomputed on the CPU by the oracle from the returned x, and a
-solution within 1e-7 relative L2 of the oracle's CG solution when both are
-driven to 1e-11.  The point of the method -- far fewer iterations than
+solution within 1e-6 relative L2 (the bar for fields) of the oracle's CG
+solution when both are driven to 1e-10 (at 1e-11 the reference's absolute
+1e-30 test on p.Ap already ends its CG in Breakdown on these systems).  The point of the method -- far fewer iterations than
 Jacobi-PCG -- is asserted too.
 """
 import numpy as np
@@ -53,11 +54,14 @@ def test_learned_reaches_tolerance_in_few_iterations(ctx, dim, n):
 def test_learned_solution_matches_oracle(ctx, dim, n):
     from cfdapp_b200.cfdb import POperator
     case, fc, diag, off, b = O.isolated_pprime(dim, n)
-    ref = O.stencil_solve(case, diag, off, b, rel_tol=1e-11, history=False)
+    ref = O.stencil_solve(case, diag, off, b, rel_tol=1e-10, history=False)
     op = POperator(ctx, dim, [n] * dim)
-    res = op.solve(b, _settings(relative_tolerance=1e-11))
+    res = op.solve(b, _settings(relative_tolerance=1e-10))
     assert res.status == ref.status == "Converged"
-    assert _rel(res.solution, ref.solution) <= 1e-7
+    assert _rel(res.solution, ref.solution) <= 1e-6
+    # tighter than the reference can go: FCG keeps converging
+    tight = op.solve(b, _settings(relative_tolerance=1e-12))
+    assert tight.status == "Converged" and tight.fallback_iterations == 0
 
 
 def test_learned_face_operator_non_square(ctx):
