@@ -4,11 +4,19 @@
 // round trip; the last kernel of each iteration decides whether another one
 // follows).
 //
-// Work layout.  Fine levels run one thread per cell, x fastest (coalesced),
-// blocks over (x-segment, row) with rows = ny*nz; neighbour reads go through
-// L1/L2, so DRAM sees each array about once per kernel.  All levels at or
-// below 4096 cells run inside ONE thread block with the level data in shared
-// memory (about 130 KB), which removes a dozen launches per cycle.
+// Work layout.  Everything runs in kernel space (2D grids as nx x 1 x ny).
+// Fine levels use plane-marching tiles: a 256-thread block owns a 32x8 (3D)
+// or 256x1 (2D) patch of an (x,y) plane and marches along z through a run of
+// planes, staging each plane with a one-cell halo in shared memory, so every
+// array is read from DRAM about once per pass and neighbours come from
+// shared memory.  Residual passes use the 7-point cross (z-neighbours kept in
+// registers); smoothing passes use the 27-point (9-point in 2D) convolution
+// over a three-plane ring.  The restriction to the next level is fused into
+// the last residual pass of a level: plane runs start on even planes, so the
+// 2x2x2 children of a coarse cell are summed inside one block (shuffle in x,
+// shared memory in y, a register across the z pair) -- deterministic, no
+// atomics.  All levels at or below 4096 cells run inside ONE thread block
+// with their data in shared memory.
 //
 // Reductions are deterministic without a grid barrier: every block stores its
 // partial sums, and the last block to finish (atomic ticket) adds all partials
@@ -71,20 +79,33 @@ MgHierarchy::~MgHierarchy() {
 
 namespace {
 
-constexpr int kMaxBlocks = 148 * 16;
+constexpr int kT = 256;                 // threads of the tiled kernels
+constexpr int kGridCap = 148 * 8;       // their blocks (8 x 256 threads resident per SM)
+constexpr int kMaxBlocks = 148 * 16;    // widest reduction launch
 constexpr int64_t kCoarseCells = 4096;
 constexpr int kMaxCoarse = 8;
 constexpr int kCoarseThreads = 1024;
 constexpr size_t kCoarseSmemCap = 200 * 1024;
 
+template <int DIM>
+struct Tile;
+template <>
+struct Tile<2> {
+  static constexpr int PX = 256, PY = 1;
+};
+template <>
+struct Tile<3> {
+  static constexpr int PX = 32, PY = 8;
+};
+
 struct Kern {
-  float w[kMgTaps];
+  float w[kMgTaps];  // kernel-space taps: (dk+1)*9 + (dj+1)*3 + (di+1)
 };
 
 struct LV {
   int nx, ny, nz;
   const float* fx;
-  const float* fy;
+  const float* fy;  // null in 2D
   const float* fz;
   const float* isq;
 };
@@ -93,9 +114,18 @@ __host__ __device__ inline LV lv(const MgLevel& M) {
   return LV{M.n[0], M.n[1], M.n[2], M.f[0], M.f[1], M.f[2], M.isq};
 }
 
+// Level-l kernel in kernel space.  A 2D weight set holds its 3x3 taps in the
+// middle plane of the 27 (real (dj, di)); kernel space maps real y to z.
 Kern kern_of(const MgWeights& W, int l) {
+  const float* w = W.w[std::min(l, W.levels - 1)];
   Kern K;
-  std::memcpy(K.w, W.w[std::min(l, W.levels - 1)], sizeof(K.w));
+  if (W.dim == 3) {
+    std::memcpy(K.w, w, sizeof(K.w));
+  } else {
+    std::memset(K.w, 0, sizeof(K.w));
+    for (int dj = 0; dj < 3; ++dj)
+      for (int di = 0; di < 3; ++di) K.w[dj * 9 + 3 + di] = w[9 + dj * 3 + di];
+  }
   return K;
 }
 float cw_of(const MgWeights& W, int l) { return W.c[std::min(l, W.levels - 1)]; }
@@ -104,53 +134,35 @@ __device__ __forceinline__ int64_t at(const LV& L, int i, int j, int k) {
   return i + (int64_t)L.nx * (j + (int64_t)L.ny * k);
 }
 
-// (A_l x) at (i,j,k); x(q, i, j, k) returns x at linear cell q with
-// coordinates (i,j,k).  Boundary face coefficients enter the diagonal only.
-template <int DIM, class X>
-__device__ __forceinline__ float lap(const LV& L, int i, int j, int k, X x) {
-  const int64_t c = at(L, i, j, k);
+struct C7 {
+  float xl, xh, yl, yh, zl, zh, d;
+};
+
+// Face couplings of cell (i,j,k); boundary faces enter the diagonal only
+// (their neighbour values are 0 in every caller).
+template <int DIM>
+__device__ __forceinline__ C7 coef(const LV& L, int i, int j, int k) {
+  C7 c;
   const int64_t bx = i + (int64_t)(L.nx + 1) * (j + (int64_t)L.ny * k);
-  const int64_t by = i + (int64_t)L.nx * (j + (int64_t)(L.ny + 1) * k);
-  const float axl = L.fx[bx], axh = L.fx[bx + 1], ayl = L.fy[by], ayh = L.fy[by + L.nx];
-  float d = (axl + axh) + (ayl + ayh);
-  float off = 0.f;
-  if (i > 0) off += axl * x(c - 1, i - 1, j, k);
-  if (i + 1 < L.nx) off += axh * x(c + 1, i + 1, j, k);
-  if (j > 0) off += ayl * x(c - L.nx, i, j - 1, k);
-  if (j + 1 < L.ny) off += ayh * x(c + L.nx, i, j + 1, k);
+  c.xl = L.fx[bx];
+  c.xh = L.fx[bx + 1];
   if (DIM == 3) {
-    const int64_t plane = (int64_t)L.nx * L.ny;
-    const float azl = L.fz[c], azh = L.fz[c + plane];
-    d += azl + azh;
-    if (k > 0) off += azl * x(c - plane, i, j, k - 1);
-    if (k + 1 < L.nz) off += azh * x(c + plane, i, j, k + 1);
+    const int64_t by = i + (int64_t)L.nx * (j + (int64_t)(L.ny + 1) * k);
+    c.yl = L.fy[by];
+    c.yh = L.fy[by + L.nx];
+  } else {
+    c.yl = c.yh = 0.f;
   }
-  return d * x(c, i, j, k) - off;
+  const int64_t bz = at(L, i, j, k);
+  c.zl = L.fz[bz];
+  c.zh = L.fz[bz + (int64_t)L.nx * L.ny];
+  c.d = ((c.xl + c.xh) + (c.yl + c.yh)) + (c.zl + c.zh);
+  return c;
 }
 
-// isq(c) * sum_o W[o] isq(c+o) v(c+o): the learned smoothing convolution.
-template <int DIM, class V>
-__device__ __forceinline__ float conv(const LV& L, const Kern& K, int i, int j, int k, V v) {
-  float s = 0.f;
-#pragma unroll
-  for (int dk = -1; dk <= 1; ++dk) {
-    if (DIM == 2 && dk != 0) continue;
-    const int kk = k + dk;
-    if (kk < 0 || kk >= L.nz) continue;
-#pragma unroll
-    for (int dj = -1; dj <= 1; ++dj) {
-      const int jj = j + dj;
-      if (jj < 0 || jj >= L.ny) continue;
-#pragma unroll
-      for (int di = -1; di <= 1; ++di) {
-        const int ii = i + di;
-        if (ii < 0 || ii >= L.nx) continue;
-        const int64_t q = at(L, ii, jj, kk);
-        s += K.w[(dk + 1) * 9 + (dj + 1) * 3 + (di + 1)] * (L.isq[q] * v(q));
-      }
-    }
-  }
-  return L.isq[at(L, i, j, k)] * s;
+__device__ __forceinline__ float apply7(const C7& c, float v, float w, float e, float s, float n,
+                                        float b, float t) {
+  return c.d * v - (((c.xl * w + c.xh * e) + (c.yl * s + c.yh * n)) + (c.zl * b + c.zh * t));
 }
 
 // Parent (coarse) cell of fine cell (i,j,k).
@@ -158,24 +170,125 @@ __device__ __forceinline__ int64_t parent(const LV& C, int i, int j, int k) {
   return (i >> 1) + (int64_t)C.nx * ((j >> 1) + (int64_t)C.ny * (k >> 1));
 }
 
-// ------------------------------------------------------------- launch shape
+// ------------------------------------------------------- tiled plane march
 
-struct Shape {
-  dim3 grid, block;
+// Work of a tiled pass: tiles x plane pairs; block b takes a contiguous run
+// of pair items, so its plane runs start on even planes.
+struct Seg {
+  int tiles_x;
+  int pairs;
+  int64_t items;
 };
 
-Shape cells_shape(int nx, int64_t rows) {
-  const int bx = nx >= 96 ? 128 : (nx >= 48 ? 64 : 32);
-  const int gx = (nx + bx - 1) / bx;
-  const int64_t gy = std::max<int64_t>(1, std::min<int64_t>(rows, std::max(1, kMaxBlocks / gx)));
-  return Shape{dim3(gx, (unsigned)gy), dim3(bx)};
+template <int DIM>
+Seg make_seg(int nx, int ny, int nz) {
+  Seg s;
+  s.tiles_x = (nx + Tile<DIM>::PX - 1) / Tile<DIM>::PX;
+  const int64_t tiles = (int64_t)s.tiles_x * ((ny + Tile<DIM>::PY - 1) / Tile<DIM>::PY);
+  s.pairs = (nz + 1) / 2;
+  s.items = tiles * s.pairs;
+  return s;
 }
 
+int seg_grid(const Seg& s) { return (int)std::max<int64_t>(1, std::min<int64_t>(s.items, kGridCap)); }
+
+// f(tix, tiy, k0, k1) for every plane run of this block.
 template <class F>
-__device__ __forceinline__ void each_cell(int nx, int ny, int rows, F f) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nx) return;
-  for (int row = blockIdx.y; row < rows; row += gridDim.y) f(i, row % ny, row / ny, (int64_t)row * nx + i);
+__device__ __forceinline__ void for_runs(const Seg& sg, int nz, F f) {
+  const int64_t w0 = sg.items * blockIdx.x / gridDim.x;
+  const int64_t w1 = sg.items * (blockIdx.x + 1) / gridDim.x;
+  int64_t w = w0;
+  while (w < w1) {
+    const int64_t tile = w / sg.pairs;
+    const int kp0 = (int)(w % sg.pairs);
+    const int kp1 = (int)min((int64_t)sg.pairs, kp0 + (w1 - w));
+    f((int)(tile % sg.tiles_x), (int)(tile / sg.tiles_x), 2 * kp0, min(nz, 2 * kp1));
+    w += kp1 - kp0;
+  }
+}
+
+// 7-point march: val(i,j,k) is the stencil input; cell(act, i, j, k, v, w, e,
+// s, n, b, t) runs in EVERY thread for every plane (act: the thread owns an
+// in-domain cell), so it may use warp and block collectives.
+template <typename T, int PX, int PY, class Val, class Cell>
+__device__ __forceinline__ void march7(int nx, int ny, int nz, int tix, int tiy, int k0, int k1,
+                                       T (*buf)[PY + 2][PX + 2], Val val, Cell cell) {
+  const int tx = threadIdx.x % PX, ty = threadIdx.x / PX;
+  const int i = tix * PX + tx, j = tiy * PY + ty;
+  const bool act = i < nx && j < ny;
+  T vprev = T(0), vcur = T(0);
+  if (act) {
+    if (k0 > 0) vprev = val(i, j, k0 - 1);
+    vcur = val(i, j, k0);
+  }
+  for (int k = k0; k < k1; ++k) {
+    const T vnext = (act && k + 1 < nz) ? val(i, j, k + 1) : T(0);
+    T(*s)[PX + 2] = buf[k & 1];
+    s[ty + 1][tx + 1] = vcur;
+    if (tx == 0) s[ty + 1][0] = (i > 0 && j < ny) ? val(i - 1, j, k) : T(0);
+    if (tx == PX - 1) s[ty + 1][PX + 1] = (i + 1 < nx && j < ny) ? val(i + 1, j, k) : T(0);
+    if (PY > 1) {
+      if (ty == 0) s[0][tx + 1] = (j > 0 && i < nx) ? val(i, j - 1, k) : T(0);
+      if (ty == PY - 1) s[PY + 1][tx + 1] = (j + 1 < ny && i < nx) ? val(i, j + 1, k) : T(0);
+    }
+    __syncthreads();
+    const T vs = (PY > 1) ? s[ty][tx + 1] : T(0);
+    const T vn = (PY > 1) ? s[ty + 2][tx + 1] : T(0);
+    cell(act, i, j, k, vcur, s[ty + 1][tx], s[ty + 1][tx + 2], vs, vn, vprev, vnext);
+    vprev = vcur;
+    vcur = vnext;
+  }
+  __syncthreads();
+}
+
+// 27-point (2D: 9-point) convolution march over a three-plane ring:
+// u(i,j,k) is the convolved field, cell(act, i, j, k, sum) runs in every
+// thread for every plane with sum = sum_o K[o] u(c+o) (0 outside the domain).
+template <int PX, int PY, bool TWO_D, class U, class Cell>
+__device__ __forceinline__ void march27(int nx, int ny, int nz, int tix, int tiy, int k0, int k1,
+                                        float (*ring)[PY + 2][PX + 2], const Kern& K, U u,
+                                        Cell cell) {
+  const int tid = threadIdx.x;
+  const int tx = tid % PX, ty = tid / PX;
+  const int i = tix * PX + tx, j = tiy * PY + ty;
+  const bool act = i < nx && j < ny;
+  auto load = [&](int kp) {
+    float(*s)[PX + 2] = ring[(kp + 3) % 3];
+    if (TWO_D) {
+      for (int q = tid; q < PX + 2; q += PX * PY) {
+        const int gi = tix * PX + q - 1;
+        s[1][q] = (kp >= 0 && kp < nz && gi >= 0 && gi < nx) ? u(gi, 0, kp) : 0.f;
+      }
+    } else {
+      for (int q = tid; q < (PY + 2) * (PX + 2); q += PX * PY) {
+        const int hy = q / (PX + 2), hx = q % (PX + 2);
+        const int gi = tix * PX + hx - 1, gj = tiy * PY + hy - 1;
+        s[hy][hx] = (kp >= 0 && kp < nz && gi >= 0 && gi < nx && gj >= 0 && gj < ny)
+                        ? u(gi, gj, kp)
+                        : 0.f;
+      }
+    }
+  };
+  load(k0 - 1);
+  load(k0);
+  for (int k = k0; k < k1; ++k) {
+    load(k + 1);
+    __syncthreads();
+    float sum = 0.f;
+    if (act) {
+#pragma unroll
+      for (int dk = -1; dk <= 1; ++dk) {
+        const float(*s)[PX + 2] = ring[(k + dk + 3) % 3];
+#pragma unroll
+        for (int dj = (TWO_D ? 0 : -1); dj <= (TWO_D ? 0 : 1); ++dj)
+#pragma unroll
+          for (int di = -1; di <= 1; ++di)
+            sum += K.w[(dk + 1) * 9 + (dj + 1) * 3 + (di + 1)] * s[ty + 1 + dj][tx + 1 + di];
+      }
+    }
+    cell(act, i, j, k, sum);
+    __syncthreads();
+  }
 }
 
 // ----------------------------------------------------------------- FCG state
@@ -224,7 +337,6 @@ __device__ __forceinline__ void reduce_last(double (&v)[NV], double* partials, u
   }
 }
 
-
 // The WHILE node's condition, or nothing when the kernels run outside a
 // graph (stream mode: active = 0).
 struct Loop {
@@ -251,49 +363,83 @@ struct Hook {
 
 // ------------------------------------------------------------ level kernels
 
-template <int DIM>
-__global__ void k_first(LV L, Kern K, const float* __restrict__ r, float* __restrict__ x,
-                        int64_t skip) {
-  each_cell(L.nx, L.ny, L.ny * L.nz, [&](int i, int j, int k, int64_t c) {
-    x[c] = conv<DIM>(L, K, i, j, k, [&](int64_t q) { return q == skip ? 0.f : r[q]; });
+// res = r - A x  (PRO: x + cw P ec in place of x).  RESTRICT: instead of
+// storing res, rc(parent) = sum of the children's res.  r[skip] reads as 0.
+template <int DIM, bool PRO, bool RESTRICT>
+__global__ void __launch_bounds__(kT) k_res(LV L, LV C, Seg sg, const float* __restrict__ x,
+                                            const float* __restrict__ ec, float cw,
+                                            const float* __restrict__ r, float* __restrict__ res,
+                                            float* __restrict__ rc, int64_t skip) {
+  constexpr int PX = Tile<DIM>::PX, PY = Tile<DIM>::PY;
+  __shared__ float buf[2][PY + 2][PX + 2];
+  __shared__ float rows[PY][PX / 2];
+  const int tx = threadIdx.x % PX, ty = threadIdx.x / PX;
+  auto val = [&](int i, int j, int k) {
+    float v = x[at(L, i, j, k)];
+    if (PRO) v += cw * ec[parent(C, i, j, k)];
+    return v;
+  };
+  for_runs(sg, L.nz, [&](int tix, int tiy, int k0, int k1) {
+    float racc = 0.f;
+    march7<float, PX, PY>(
+        L.nx, L.ny, L.nz, tix, tiy, k0, k1, buf, val,
+        [&](bool act, int i, int j, int k, float v, float w, float e, float s, float n, float b,
+            float t) {
+          float rv = 0.f;
+          if (act) {
+            const int64_t c = at(L, i, j, k);
+            rv = (c == skip ? 0.f : r[c]) - apply7(coef<DIM>(L, i, j, k), v, w, e, s, n, b, t);
+            if (!RESTRICT) res[c] = rv;
+          }
+          if (RESTRICT) {
+            const float xs = rv + __shfl_xor_sync(0xffffffffu, rv, 1);
+            float quad = xs;
+            if (PY > 1) {
+              if ((tx & 1) == 0) rows[ty][tx >> 1] = xs;
+              __syncthreads();
+              if ((tx & 1) == 0 && (ty & 1) == 0) quad = xs + rows[ty + 1][tx >> 1];
+            }
+            racc = ((k & 1) == 0) ? quad : racc + quad;
+            const bool writer = (tx & 1) == 0 && (PY == 1 || (ty & 1) == 0);
+            if (writer && ((k & 1) == 1 || k + 1 == L.nz)) {
+              const int ci = i >> 1, cj = j >> 1, ck = k >> 1;
+              if (ci < C.nx && cj < C.ny) rc[ci + (int64_t)C.nx * (cj + (int64_t)C.ny * ck)] = racc;
+            }
+          }
+        });
   });
 }
 
-template <int DIM>
-__global__ void k_resid(LV L, const float* __restrict__ x, const float* __restrict__ r,
-                        float* __restrict__ res, int64_t skip) {
-  each_cell(L.nx, L.ny, L.ny * L.nz, [&](int i, int j, int k, int64_t c) {
-    res[c] = (c == skip ? 0.f : r[c]) -
-             lap<DIM>(L, i, j, k, [&](int64_t q, int, int, int) { return x[q]; });
-  });
-}
+enum { SM_FIRST = 0, SM_ADD = 1 };
 
-// res = r - A (x + cw P ec)
-template <int DIM>
-__global__ void k_prolong_resid(LV L, LV C, const float* __restrict__ ec, float cw,
-                                const float* __restrict__ x, const float* __restrict__ r,
-                                float* __restrict__ res, int64_t skip) {
-  each_cell(L.nx, L.ny, L.ny * L.nz, [&](int i, int j, int k, int64_t c) {
-    auto xv = [&](int64_t q, int qi, int qj, int qk) {
-      return x[q] + cw * ec[parent(C, qi, qj, qk)];
-    };
-    res[c] = (c == skip ? 0.f : r[c]) - lap<DIM>(L, i, j, k, xv);
-  });
-}
-
-// x <- x (+ cw P ec) + S res; at level 0 the last sweep also pins z[skip] =
-// r[skip] and, with a hook, accumulates z.q for the FCG coefficient.
-template <int DIM, bool HOOK>
-__global__ void k_smooth(LV L, LV C, Kern K, const float* __restrict__ ec, float cw,
-                         const float* __restrict__ res, float* __restrict__ x, int64_t skip,
-                         const float* __restrict__ r, Hook hk) {
+// x <- [x] (+ cw P ec) + D^-1/2 (W * (D^-1/2 u)), u = res (SM_ADD) or r with
+// r[skip] = 0 and x = 0 before (SM_FIRST).  pin >= 0: z[pin] = r[pin] (the
+// last sweep of level 0); HOOK: also accumulate z.q for the FCG coefficient.
+template <int DIM, int MODE, bool HOOK>
+__global__ void __launch_bounds__(kT) k_sm(LV L, LV C, Seg sg, Kern K, const float* __restrict__ src,
+                                           const float* __restrict__ ec, float cw,
+                                           float* __restrict__ x, int64_t skip, int64_t pin,
+                                           const float* __restrict__ r, Hook hk) {
+  constexpr int PX = Tile<DIM>::PX, PY = Tile<DIM>::PY;
+  __shared__ float ring[3][PY + 2][PX + 2];
   double acc[1] = {0.0};
-  each_cell(L.nx, L.ny, L.ny * L.nz, [&](int i, int j, int k, int64_t c) {
-    float v = x[c] + conv<DIM>(L, K, i, j, k, [&](int64_t q) { return res[q]; });
-    if (ec) v += cw * ec[parent(C, i, j, k)];
-    if (c == skip) v = r[c];
-    x[c] = v;
-    if (HOOK) acc[0] += (double)v * hk.q[c];
+  auto u = [&](int i, int j, int k) {
+    const int64_t q = at(L, i, j, k);
+    if (MODE == SM_FIRST && q == skip) return 0.f;
+    return src[q] * L.isq[q];
+  };
+  for_runs(sg, L.nz, [&](int tix, int tiy, int k0, int k1) {
+    march27<PX, PY, DIM == 2>(L.nx, L.ny, L.nz, tix, tiy, k0, k1, ring, K, u,
+                              [&](bool act, int i, int j, int k, float sum) {
+                                if (!act) return;
+                                const int64_t c = at(L, i, j, k);
+                                float v = L.isq[c] * sum;
+                                if (MODE == SM_ADD) v += x[c];
+                                if (ec) v += cw * ec[parent(C, i, j, k)];
+                                if (c == pin) v = r[c];
+                                x[c] = v;
+                                if (HOOK) acc[0] += (double)v * hk.q[c];
+                              });
   });
   if (HOOK) {
     reduce_last<1>(acc, hk.partials, &hk.S->ticket, [&](const double* tot) {
@@ -309,34 +455,12 @@ __global__ void k_smooth(LV L, LV C, Kern K, const float* __restrict__ ec, float
   }
 }
 
-// rc(C) = sum over the children of C of (r - A x)
-template <int DIM>
-__global__ void k_resid_restrict(LV L, LV C, const float* __restrict__ x,
-                                 const float* __restrict__ r, float* __restrict__ rc, int64_t skip) {
-  each_cell(C.nx, C.ny, C.ny * C.nz, [&](int ci, int cj, int ck, int64_t qc) {
-    float s = 0.f;
-#pragma unroll
-    for (int u = 0; u < (DIM == 3 ? 2 : 1); ++u)
-#pragma unroll
-      for (int v = 0; v < 2; ++v)
-#pragma unroll
-        for (int t = 0; t < 2; ++t) {
-          const int i = 2 * ci + t, j = 2 * cj + v, k = 2 * ck + u;
-          if (i >= L.nx || j >= L.ny || k >= L.nz) continue;
-          const int64_t c = at(L, i, j, k);
-          s += (c == skip ? 0.f : r[c]) -
-               lap<DIM>(L, i, j, k, [&](int64_t q, int, int, int) { return x[q]; });
-        }
-    rc[qc] = s;
-  });
-}
-
 // ----------------------------------------------------- coarse-level block
 
 struct CoarseLevel {
   int n[3];
   int cells;
-  const float* f[3];  // global sources
+  const float* f[3];  // global sources (f[1] null in 2D)
   const float* isq;
   float* x_glob;      // global x (written back for the first coarse level)
   const float* r_glob;
@@ -352,66 +476,93 @@ struct CoarsePlan {
 };
 
 template <int DIM>
+__device__ __forceinline__ float lap_s(const LV& M, int i, int j, int k, int c, const float* x) {
+  const C7 co = coef<DIM>(M, i, j, k);
+  const int plane = M.nx * M.ny;
+  const float w = i > 0 ? x[c - 1] : 0.f, e = i + 1 < M.nx ? x[c + 1] : 0.f;
+  const float s = (DIM == 3 && j > 0) ? x[c - M.nx] : 0.f;
+  const float n = (DIM == 3 && j + 1 < M.ny) ? x[c + M.nx] : 0.f;
+  const float b = k > 0 ? x[c - plane] : 0.f, t = k + 1 < M.nz ? x[c + plane] : 0.f;
+  return apply7(co, x[c], w, e, s, n, b, t);
+}
+
+// sum_o K[o] isq(c+o) v(c+o)
+template <int DIM>
+__device__ __forceinline__ float conv_s(const LV& M, const Kern& K, int i, int j, int k,
+                                        const float* v) {
+  float s = 0.f;
+  for (int dk = -1; dk <= 1; ++dk) {
+    const int kk = k + dk;
+    if (kk < 0 || kk >= M.nz) continue;
+    for (int dj = (DIM == 2 ? 0 : -1); dj <= (DIM == 2 ? 0 : 1); ++dj) {
+      const int jj = j + dj;
+      if (jj < 0 || jj >= M.ny) continue;
+      for (int di = -1; di <= 1; ++di) {
+        const int ii = i + di;
+        if (ii < 0 || ii >= M.nx) continue;
+        const int q = ii + M.nx * (jj + M.ny * kk);
+        s += K.w[(dk + 1) * 9 + (dj + 1) * 3 + (di + 1)] * (M.isq[q] * v[q]);
+      }
+    }
+  }
+  return s;
+}
+
+template <int DIM>
 __global__ void __launch_bounds__(kCoarseThreads) k_coarse(CoarsePlan P) {
   extern __shared__ float4 smem4[];
   float* sm = reinterpret_cast<float*>(smem4);
   const int tid = threadIdx.x, nt = blockDim.x;
-  // stage the levels' coefficients into shared memory
   for (int l = 0; l < P.count; ++l) {
     const CoarseLevel& c = P.lv[l];
     const int nf[3] = {(c.n[0] + 1) * c.n[1] * c.n[2], c.n[0] * (c.n[1] + 1) * c.n[2],
-                       DIM == 3 ? c.n[0] * c.n[1] * (c.n[2] + 1) : 0};
-    for (int a = 0; a < DIM; ++a)
+                       c.n[0] * c.n[1] * (c.n[2] + 1)};
+    for (int a = 0; a < 3; ++a) {
+      if (DIM == 2 && a == 1) continue;
       for (int q = tid; q < nf[a]; q += nt) sm[c.off[a] + q] = c.f[a][q];
+    }
     for (int q = tid; q < c.cells; q += nt) sm[c.off[3] + q] = c.isq[q];
   }
   for (int q = tid; q < P.lv[0].cells; q += nt) sm[P.lv[0].off[5] + q] = P.lv[0].r_glob[q];
   __syncthreads();
   auto level = [&](int l) {
     const CoarseLevel& c = P.lv[l];
-    return LV{c.n[0], c.n[1], c.n[2], sm + c.off[0], sm + c.off[1],
-              DIM == 3 ? sm + c.off[2] : nullptr, sm + c.off[3]};
+    return LV{c.n[0], c.n[1], c.n[2], sm + c.off[0], DIM == 3 ? sm + c.off[1] : nullptr,
+              sm + c.off[2], sm + c.off[3]};
   };
-  auto X = [&](int l) { return sm + P.lv[l].off[4]; };
-  auto R = [&](int l) { return sm + P.lv[l].off[5]; };
-  auto RES = [&](int l) { return sm + P.lv[l].off[6]; };
-  auto cell_loop = [&](const LV& M, auto f) {
+  auto cells_of = [&](const LV& M, auto f) {
     const int cells = M.nx * M.ny * M.nz;
     for (int c = tid; c < cells; c += nt) {
       const int i = c % M.nx, rest = c / M.nx;
       f(i, rest % M.ny, rest / M.ny, c);
     }
   };
-  auto xval = [](const float* x) { return [x](int64_t q, int, int, int) { return x[q]; }; };
   const int last = P.count - 1;
   for (int l = 0; l < last; ++l) {
     const LV M = level(l);
-    float* x = X(l);
-    const float* r = R(l);
-    float* res = RES(l);
-    cell_loop(M, [&](int i, int j, int k, int c) {
-      x[c] = conv<DIM>(M, P.K[l], i, j, k, [&](int64_t q) { return r[q]; });
-    });
+    float* x = sm + P.lv[l].off[4];
+    const float* r = sm + P.lv[l].off[5];
+    float* res = sm + P.lv[l].off[6];
+    const Kern& K = P.K[l];
+    cells_of(M, [&](int i, int j, int k, int c) { x[c] = M.isq[c] * conv_s<DIM>(M, K, i, j, k, r); });
     __syncthreads();
     for (int s = 1; s < P.nu; ++s) {
-      cell_loop(M, [&](int i, int j, int k, int c) { res[c] = r[c] - lap<DIM>(M, i, j, k, xval(x)); });
+      cells_of(M, [&](int i, int j, int k, int c) { res[c] = r[c] - lap_s<DIM>(M, i, j, k, c, x); });
       __syncthreads();
-      cell_loop(M, [&](int i, int j, int k, int c) {
-        x[c] += conv<DIM>(M, P.K[l], i, j, k, [&](int64_t q) { return res[q]; });
-      });
+      cells_of(M, [&](int i, int j, int k, int c) { x[c] += M.isq[c] * conv_s<DIM>(M, K, i, j, k, res); });
       __syncthreads();
     }
-    cell_loop(M, [&](int i, int j, int k, int c) { res[c] = r[c] - lap<DIM>(M, i, j, k, xval(x)); });
+    cells_of(M, [&](int i, int j, int k, int c) { res[c] = r[c] - lap_s<DIM>(M, i, j, k, c, x); });
     __syncthreads();
     const LV Cc = level(l + 1);
-    float* rc = R(l + 1);
-    cell_loop(Cc, [&](int ci, int cj, int ck, int qc) {
+    float* rc = sm + P.lv[l + 1].off[5];
+    cells_of(Cc, [&](int ci, int cj, int ck, int qc) {
       float s = 0.f;
-      for (int u = 0; u < (DIM == 3 ? 2 : 1); ++u)
+      for (int u = 0; u < 2; ++u)
         for (int v = 0; v < 2; ++v)
           for (int t = 0; t < 2; ++t) {
             const int i = 2 * ci + t, j = 2 * cj + v, k = 2 * ck + u;
-            if (i < M.nx && j < M.ny && k < M.nz) s += res[at(M, i, j, k)];
+            if (i < M.nx && j < M.ny && k < M.nz) s += res[i + M.nx * (j + M.ny * k)];
           }
       rc[qc] = s;
     });
@@ -419,15 +570,15 @@ __global__ void __launch_bounds__(kCoarseThreads) k_coarse(CoarsePlan P) {
   }
   {
     const LV M = level(last);
-    float* x = X(last);
-    const float* r = R(last);
-    float* res = RES(last);
-    cell_loop(M, [&](int, int, int, int c) { x[c] = 0.f; });
+    float* x = sm + P.lv[last].off[4];
+    const float* r = sm + P.lv[last].off[5];
+    float* res = sm + P.lv[last].off[6];
+    cells_of(M, [&](int, int, int, int c) { x[c] = 0.f; });
     __syncthreads();
     for (int s = 0; s < P.sweeps; ++s) {
-      cell_loop(M, [&](int i, int j, int k, int c) { res[c] = r[c] - lap<DIM>(M, i, j, k, xval(x)); });
+      cells_of(M, [&](int i, int j, int k, int c) { res[c] = r[c] - lap_s<DIM>(M, i, j, k, c, x); });
       __syncthreads();
-      cell_loop(M, [&](int, int, int, int c) {
+      cells_of(M, [&](int, int, int, int c) {
         const float is = M.isq[c];
         x[c] += 0.8f * (is * is) * res[c];
       });
@@ -437,33 +588,22 @@ __global__ void __launch_bounds__(kCoarseThreads) k_coarse(CoarsePlan P) {
   for (int l = last - 1; l >= 0; --l) {
     const LV M = level(l);
     const LV Cc = level(l + 1);
-    float* x = X(l);
-    const float* r = R(l);
-    float* res = RES(l);
-    const float* ec = X(l + 1);
+    float* x = sm + P.lv[l].off[4];
+    const float* r = sm + P.lv[l].off[5];
+    float* res = sm + P.lv[l].off[6];
+    const float* ec = sm + P.lv[l + 1].off[4];
     const float cw = P.cw[l];
-    cell_loop(M, [&](int i, int j, int k, int c) {
-      auto xv = [&](int64_t q, int qi, int qj, int qk) {
-        return x[q] + cw * ec[parent(Cc, qi, qj, qk)];
-      };
-      res[c] = r[c] - lap<DIM>(M, i, j, k, xv);
-    });
+    const Kern& K = P.K[l];
+    cells_of(M, [&](int i, int j, int k, int c) { x[c] += cw * ec[parent(Cc, i, j, k)]; });
     __syncthreads();
-    cell_loop(M, [&](int i, int j, int k, int c) {
-      x[c] += cw * ec[parent(Cc, i, j, k)] +
-              conv<DIM>(M, P.K[l], i, j, k, [&](int64_t q) { return res[q]; });
-    });
-    __syncthreads();
-    for (int s = 1; s < P.nu; ++s) {
-      cell_loop(M, [&](int i, int j, int k, int c) { res[c] = r[c] - lap<DIM>(M, i, j, k, xval(x)); });
+    for (int s = 0; s < P.nu; ++s) {
+      cells_of(M, [&](int i, int j, int k, int c) { res[c] = r[c] - lap_s<DIM>(M, i, j, k, c, x); });
       __syncthreads();
-      cell_loop(M, [&](int i, int j, int k, int c) {
-        x[c] += conv<DIM>(M, P.K[l], i, j, k, [&](int64_t q) { return res[q]; });
-      });
+      cells_of(M, [&](int i, int j, int k, int c) { x[c] += M.isq[c] * conv_s<DIM>(M, K, i, j, k, res); });
       __syncthreads();
     }
   }
-  for (int q = tid; q < P.lv[0].cells; q += nt) P.lv[0].x_glob[q] = X(0)[q];
+  for (int q = tid; q < P.lv[0].cells; q += nt) P.lv[0].x_glob[q] = sm[P.lv[0].off[4] + q];
 }
 
 // ------------------------------------------------------ hierarchy build
@@ -519,27 +659,29 @@ __global__ void k_agglomerate(MgLevel F, MgLevel C, int a) {
 template <int DIM>
 __global__ void k_isq(MgLevel M) {
   const LV L = lv(M);
-  each_cell(L.nx, L.ny, L.ny * L.nz, [&](int i, int j, int k, int64_t c) {
-    const float d = lap<DIM>(L, i, j, k, [&](int64_t q, int, int, int) { return q == c ? 1.f : 0.f; });
-    M.isq[c] = d > 0.f ? rsqrtf(d) : 0.f;
-  });
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < M.cells;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(q % L.nx);
+    const int64_t rest = q / L.nx;
+    const int j = (int)(rest % L.ny), k = (int)(rest / L.ny);
+    const float d = coef<DIM>(L, i, j, k).d;
+    M.isq[q] = d > 0.f ? rsqrtf(d) : 0.f;
+  }
 }
 
 int flat_grid(int64_t n) {
   return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, kMaxBlocks));
 }
 
-template <int DIM>
-void launch_isq(const MgLevel& M, cudaStream_t st) {
-  const Shape s = cells_shape(M.n[0], (int64_t)M.n[1] * M.n[2]);
-  k_isq<DIM><<<s.grid, s.block, 0, st>>>(M);
-}
+bool axis_active(int dim, int a) { return dim == 3 || a != 1; }
 
 cfdb_status refresh_values(cfdb_context* ctx, MgHierarchy& H, const FineOperator& op) {
   cudaStream_t st = ctx->stream;
+  int launches = 0;
   for (int l = 0; l < H.levels; ++l) {
     MgLevel& M = H.L[l];
-    for (int a = 0; a < H.dim; ++a) {
+    for (int a = 0; a < 3; ++a) {
+      if (!axis_active(H.dim, a)) continue;
       int e[3] = {M.n[0], M.n[1], M.n[2]};
       e[a] += 1;
       const int64_t m = (int64_t)e[0] * e[1] * e[2];
@@ -547,12 +689,14 @@ cfdb_status refresh_values(cfdb_context* ctx, MgHierarchy& H, const FineOperator
         k_faces0<<<flat_grid(m), 256, 0, st>>>(M.f[a], e[0], e[1], e[2], a, op.full[a], op.table[a]);
       else
         k_agglomerate<<<flat_grid(m), 256, 0, st>>>(H.L[l - 1], M, a);
+      ++launches;
     }
-    if (H.dim == 2) launch_isq<2>(M, st);
-    else launch_isq<3>(M, st);
+    if (H.dim == 2) k_isq<2><<<flat_grid(M.cells), 256, 0, st>>>(M);
+    else k_isq<3><<<flat_grid(M.cells), 256, 0, st>>>(M);
+    ++launches;
   }
   CFDB_CHECK_LAUNCH(ctx);
-  count_launch(ctx, H.levels * (H.dim + 1));
+  count_launch(ctx, launches);
   return CFDB_OK;
 }
 
@@ -564,8 +708,8 @@ size_t coarse_bytes(const MgHierarchy& H, int from) {
   size_t floats = 0;
   for (int l = from; l < H.levels; ++l) {
     const MgLevel& M = H.L[l];
-    floats += up4((int64_t)(M.n[0] + 1) * M.n[1] * M.n[2]) + up4((int64_t)M.n[0] * (M.n[1] + 1) * M.n[2]);
-    if (H.dim == 3) floats += up4((int64_t)M.n[0] * M.n[1] * (M.n[2] + 1));
+    floats += up4((int64_t)(M.n[0] + 1) * M.n[1] * M.n[2]) + up4((int64_t)M.n[0] * M.n[1] * (M.n[2] + 1));
+    if (H.dim == 3) floats += up4((int64_t)M.n[0] * (M.n[1] + 1) * M.n[2]);
     floats += 4 * up4(M.cells);
   }
   return floats * sizeof(float);
@@ -593,8 +737,8 @@ CoarsePlan coarse_plan(const MgHierarchy& H, const MgWeights& W) {
     c.x_glob = M.x;
     c.r_glob = M.r;
     c.off[0] = take((int64_t)(c.n[0] + 1) * c.n[1] * c.n[2]);
-    c.off[1] = take((int64_t)c.n[0] * (c.n[1] + 1) * c.n[2]);
-    c.off[2] = H.dim == 3 ? take((int64_t)c.n[0] * c.n[1] * (c.n[2] + 1)) : 0;
+    c.off[1] = H.dim == 3 ? take((int64_t)c.n[0] * (c.n[1] + 1) * c.n[2]) : 0;
+    c.off[2] = take((int64_t)c.n[0] * c.n[1] * (c.n[2] + 1));
     for (int s = 3; s < 7; ++s) c.off[s] = take(c.cells);
     P.K[q] = kern_of(W, H.coarse_from + q);
     P.cw[q] = cw_of(W, H.coarse_from + q);
@@ -613,21 +757,23 @@ int enqueue_cycle(const MgHierarchy& H, const MgWeights& W, const float* r0, flo
   auto xp = [&](int l) -> float* { return l == 0 ? z0 : H.L[l].x; };
   for (int l = 0; l < cf; ++l) {
     const MgLevel& M = H.L[l];
-    const LV L = lv(M);
+    const LV L = lv(M), LC = lv(H.L[l + 1]);
     const Kern K = kern_of(W, l);
     const int64_t sk = l == 0 ? skip : -1;
-    const Shape s = cells_shape(M.n[0], (int64_t)M.n[1] * M.n[2]);
-    k_first<DIM><<<s.grid, s.block, 0, st>>>(L, K, rp(l), xp(l), sk);
+    const Seg sg = make_seg<DIM>(M.n[0], M.n[1], M.n[2]);
+    const int g = seg_grid(sg);
+    k_sm<DIM, SM_FIRST, false><<<g, kT, 0, st>>>(L, LC, sg, K, rp(l), nullptr, 0.f, xp(l), sk, -1,
+                                                 nullptr, Hook{});
     ++launches;
     for (int q = 1; q < W.nu; ++q) {
-      k_resid<DIM><<<s.grid, s.block, 0, st>>>(L, xp(l), rp(l), M.res, sk);
-      k_smooth<DIM, false><<<s.grid, s.block, 0, st>>>(L, L, K, nullptr, 0.f, M.res, xp(l), -1,
-                                                       nullptr, Hook{});
+      k_res<DIM, false, false><<<g, kT, 0, st>>>(L, LC, sg, xp(l), nullptr, 0.f, rp(l), M.res,
+                                                 nullptr, sk);
+      k_sm<DIM, SM_ADD, false><<<g, kT, 0, st>>>(L, LC, sg, K, M.res, nullptr, 0.f, xp(l), -1, -1,
+                                                 nullptr, Hook{});
       launches += 2;
     }
-    const MgLevel& C = H.L[l + 1];
-    const Shape sc = cells_shape(C.n[0], (int64_t)C.n[1] * C.n[2]);
-    k_resid_restrict<DIM><<<sc.grid, sc.block, 0, st>>>(L, lv(C), xp(l), rp(l), C.r, sk);
+    k_res<DIM, false, true><<<g, kT, 0, st>>>(L, LC, sg, xp(l), nullptr, 0.f, rp(l), nullptr,
+                                              H.L[l + 1].r, sk);
     ++launches;
   }
   if (cf < H.levels) {
@@ -642,20 +788,23 @@ int enqueue_cycle(const MgHierarchy& H, const MgWeights& W, const float* r0, flo
     const Kern K = kern_of(W, l);
     const float cw = cw_of(W, l);
     const int64_t sk = l == 0 ? skip : -1;
-    const Shape s = cells_shape(M.n[0], (int64_t)M.n[1] * M.n[2]);
+    const Seg sg = make_seg<DIM>(M.n[0], M.n[1], M.n[2]);
+    const int g = seg_grid(sg);
     for (int q = 0; q < W.nu; ++q) {
-      if (q == 0)
-        k_prolong_resid<DIM><<<s.grid, s.block, 0, st>>>(L, LC, C.x, cw, xp(l), rp(l), M.res, sk);
-      else
-        k_resid<DIM><<<s.grid, s.block, 0, st>>>(L, xp(l), rp(l), M.res, sk);
-      const bool last = (l == 0 && q == W.nu - 1);
       const float* ec = q == 0 ? C.x : nullptr;
-      if (last && hook)
-        k_smooth<DIM, true><<<s.grid, s.block, 0, st>>>(L, LC, K, ec, cw, M.res, xp(l), sk,
-                                                        rp(l), *hook);
+      if (q == 0)
+        k_res<DIM, true, false><<<g, kT, 0, st>>>(L, LC, sg, xp(l), C.x, cw, rp(l), M.res, nullptr,
+                                                  sk);
       else
-        k_smooth<DIM, false><<<s.grid, s.block, 0, st>>>(L, LC, K, ec, cw, M.res, xp(l),
-                                                         last ? sk : -1, rp(l), Hook{});
+        k_res<DIM, false, false><<<g, kT, 0, st>>>(L, LC, sg, xp(l), nullptr, 0.f, rp(l), M.res,
+                                                   nullptr, sk);
+      const bool last = (l == 0 && q == W.nu - 1);
+      if (last && hook)
+        k_sm<DIM, SM_ADD, true><<<g, kT, 0, st>>>(L, LC, sg, K, M.res, ec, cw, xp(l), -1, sk, rp(l),
+                                                  *hook);
+      else
+        k_sm<DIM, SM_ADD, false><<<g, kT, 0, st>>>(L, LC, sg, K, M.res, ec, cw, xp(l), -1,
+                                                   last ? sk : -1, rp(l), Hook{});
       launches += 2;
     }
   }
@@ -663,7 +812,8 @@ int enqueue_cycle(const MgHierarchy& H, const MgWeights& W, const float* r0, flo
 }
 
 // Algorithmic bytes of one V-cycle: FP32 words read and written per level,
-// each array counted once per kernel.
+// each array counted once per kernel (faces: about one word per cell and
+// active axis).
 double cycle_bytes(const MgHierarchy& H, const MgWeights& W) {
   const double d = H.dim, fr = 1.0 / (H.dim == 3 ? 8.0 : 4.0);
   double words = 0.0;
@@ -681,22 +831,29 @@ double cycle_bytes(const MgHierarchy& H, const MgWeights& W) {
 // ------------------------------------------------------------ FCG kernels
 
 // r = b - A x, r32 = float(r); ||r|| decides whether the loop runs at all.
-__global__ void k_fcg_init(OpView<double> A, FcgState* S, double* __restrict__ r,
-                           float* __restrict__ r32, double* partials, double* hist, int64_t hcap,
-                           Loop h) {
+template <int DIM>
+__global__ void __launch_bounds__(kT) k_fcg_init(OpView<double> A, Seg sg, FcgState* S,
+                                                 double* __restrict__ r, float* __restrict__ r32,
+                                                 double* partials, double* hist, int64_t hcap,
+                                                 Loop h) {
+  constexpr int PX = Tile<DIM>::PX, PY = Tile<DIM>::PY;
+  __shared__ double buf[2][PY + 2][PX + 2];
   const double* __restrict__ b = S->b;
   const double* __restrict__ x = S->x;
   double acc[1] = {0.0};
-  const int64_t plane = (int64_t)A.nx * A.ny;
-  each_cell(A.nx, A.ny, A.ny * A.nz, [&](int i, int j, int k, int64_t c) {
-    const Coef<double> cf = load_coef(A, i, j, k);
-    const double w = i > 0 ? x[c - 1] : 0.0, e = i + 1 < A.nx ? x[c + 1] : 0.0;
-    const double s = j > 0 ? x[c - A.nx] : 0.0, n = j + 1 < A.ny ? x[c + A.nx] : 0.0;
-    const double bo = k > 0 ? x[c - plane] : 0.0, t = k + 1 < A.nz ? x[c + plane] : 0.0;
-    const double rn = b[c] - apply_coef(cf, x[c], w, e, s, n, bo, t);
-    r[c] = rn;
-    r32[c] = (float)rn;
-    acc[0] += rn * rn;
+  auto val = [&](int i, int j, int k) { return x[i + (int64_t)A.nx * (j + (int64_t)A.ny * k)]; };
+  for_runs(sg, A.nz, [&](int tix, int tiy, int k0, int k1) {
+    march7<double, PX, PY>(A.nx, A.ny, A.nz, tix, tiy, k0, k1, buf, val,
+                           [&](bool act, int i, int j, int k, double v, double w, double e,
+                               double s, double n, double bo, double t) {
+                             if (!act) return;
+                             const int64_t c = i + (int64_t)A.nx * (j + (int64_t)A.ny * k);
+                             const double rn =
+                                 b[c] - apply_coef(load_coef(A, i, j, k), v, w, e, s, n, bo, t);
+                             r[c] = rn;
+                             r32[c] = (float)rn;
+                             acc[0] += rn * rn;
+                           });
   });
   reduce_last<1>(acc, partials, &S->ticket, [&](const double* tot) {
     const double b0 = sqrt(tot[0]);
@@ -722,30 +879,36 @@ __global__ void k_fcg_init(OpView<double> A, FcgState* S, double* __restrict__ r
 
 // p = z - beta p_old (p = z on the first iteration), q = A p; p.q and p.r
 // give alpha.  p alternates between two buffers by iteration parity.
-__global__ void k_fcg_dir(OpView<double> A, FcgState* S, const float* __restrict__ z,
-                          double* P0, double* P1, double* __restrict__ q,
-                          const double* __restrict__ r, double* partials,
-                          Loop h) {
+template <int DIM>
+__global__ void __launch_bounds__(kT) k_fcg_dir(OpView<double> A, Seg sg, FcgState* S,
+                                                const float* __restrict__ z, double* P0, double* P1,
+                                                double* __restrict__ q, const double* __restrict__ r,
+                                                double* partials, Loop h) {
+  constexpr int PX = Tile<DIM>::PX, PY = Tile<DIM>::PY;
+  __shared__ double buf[2][PY + 2][PX + 2];
   if (S->done) return;
   const long long it = S->it;
   const bool first = (it == 0);
   const double beta = first ? 0.0 : S->beta;
   double* __restrict__ pn = (it & 1) ? P1 : P0;
   const double* __restrict__ po = (it & 1) ? P0 : P1;
-  auto pv = [&](int64_t c) { return first ? (double)z[c] : fma(-beta, po[c], (double)z[c]); };
+  auto val = [&](int i, int j, int k) {
+    const int64_t c = i + (int64_t)A.nx * (j + (int64_t)A.ny * k);
+    return first ? (double)z[c] : fma(-beta, po[c], (double)z[c]);
+  };
   double acc[2] = {0.0, 0.0};
-  const int64_t plane = (int64_t)A.nx * A.ny;
-  each_cell(A.nx, A.ny, A.ny * A.nz, [&](int i, int j, int k, int64_t c) {
-    const Coef<double> cf = load_coef(A, i, j, k);
-    const double v = pv(c);
-    const double w = i > 0 ? pv(c - 1) : 0.0, e = i + 1 < A.nx ? pv(c + 1) : 0.0;
-    const double s = j > 0 ? pv(c - A.nx) : 0.0, n = j + 1 < A.ny ? pv(c + A.nx) : 0.0;
-    const double bo = k > 0 ? pv(c - plane) : 0.0, t = k + 1 < A.nz ? pv(c + plane) : 0.0;
-    const double aq = apply_coef(cf, v, w, e, s, n, bo, t);
-    pn[c] = v;
-    q[c] = aq;
-    acc[0] += v * aq;
-    acc[1] += v * r[c];
+  for_runs(sg, A.nz, [&](int tix, int tiy, int k0, int k1) {
+    march7<double, PX, PY>(A.nx, A.ny, A.nz, tix, tiy, k0, k1, buf, val,
+                           [&](bool act, int i, int j, int k, double v, double w, double e,
+                               double s, double n, double bo, double t) {
+                             if (!act) return;
+                             const int64_t c = i + (int64_t)A.nx * (j + (int64_t)A.ny * k);
+                             const double aq = apply_coef(load_coef(A, i, j, k), v, w, e, s, n, bo, t);
+                             pn[c] = v;
+                             q[c] = aq;
+                             acc[0] += v * aq;
+                             acc[1] += v * r[c];
+                           });
   });
   reduce_last<2>(acc, partials, &S->ticket, [&](const double* tot) {
     const double pq = tot[0], pr = tot[1];
@@ -775,9 +938,8 @@ __global__ void k_fcg_update(int64_t n, FcgState* S, double* __restrict__ r,
   const double* __restrict__ p = (it & 1) ? P1 : P0;
   double* __restrict__ x = S->x;
   double acc[1] = {0.0};
-  const int64_t stride = (int64_t)gridDim.x * gridDim.y * blockDim.x;
-  for (int64_t c = (blockIdx.x + (int64_t)gridDim.x * blockIdx.y) * blockDim.x + threadIdx.x; c < n;
-       c += stride) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n; c += stride) {
     x[c] = fma(alpha, p[c], x[c]);
     const double rn = fma(-alpha, q[c], r[c]);
     r[c] = rn;
@@ -815,7 +977,7 @@ __global__ void k_fcg_update(int64_t n, FcgState* S, double* __restrict__ r,
 
 cfdb_status mg_build(cfdb_context* ctx, MgHierarchy& H, const FineOperator& op) {
   H.dim = op.dim;
-  int n[3] = {op.n[0], op.n[1], op.dim == 3 ? op.n[2] : 1};
+  int n[3] = {op.n[0], op.n[1], op.n[2]};
   int l = 0;
   auto alloc = [&](float** p, int64_t count) -> cfdb_status {
     CFDB_CUDA(ctx, cudaMalloc((void**)p, sizeof(float) * (size_t)std::max<int64_t>(count, 4)));
@@ -827,7 +989,8 @@ cfdb_status mg_build(cfdb_context* ctx, MgHierarchy& H, const FineOperator& op) 
     std::memset(&M, 0, sizeof(M));
     for (int a = 0; a < 3; ++a) M.n[a] = n[a];
     M.cells = (int64_t)n[0] * n[1] * n[2];
-    for (int a = 0; a < op.dim; ++a) {
+    for (int a = 0; a < 3; ++a) {
+      if (!axis_active(op.dim, a)) continue;
       int e[3] = {n[0], n[1], n[2]};
       e[a] += 1;
       cfdb_status rc = alloc(&M.f[a], (int64_t)e[0] * e[1] * e[2]);
@@ -839,11 +1002,13 @@ cfdb_status mg_build(cfdb_context* ctx, MgHierarchy& H, const FineOperator& op) 
     if (l > 0 && ((rc = alloc(&M.x, M.cells)) != CFDB_OK || (rc = alloc(&M.r, M.cells)) != CFDB_OK))
       return rc;
     ++l;
-    int mn = n[0];
-    for (int a = 1; a < op.dim; ++a) mn = std::min(mn, n[a]);
+    int mn = 1 << 30;
+    for (int a = 0; a < 3; ++a)
+      if (axis_active(op.dim, a)) mn = std::min(mn, n[a]);
     const bool stop = (l > 1 && (mn <= 4 || M.cells <= 64)) || mn == 1 || l == kMgMaxLevels;
     if (stop) break;
-    for (int a = 0; a < op.dim; ++a) n[a] = (n[a] + 1) / 2;
+    for (int a = 0; a < 3; ++a)
+      if (axis_active(op.dim, a)) n[a] = (n[a] + 1) / 2;
   }
   H.levels = l;
   if (H.levels < 2)
@@ -935,21 +1100,42 @@ void learned_destroy(LearnedSolver* s) {
 namespace {
 
 // Blocks of the widest reduction launch (one partial per block and value).
-int64_t partial_slots(const FineOperator& op) {
-  const Shape sh = cells_shape(op.A.nx, (int64_t)op.A.ny * op.A.nz);
-  return std::max<int64_t>((int64_t)sh.grid.x * sh.grid.y, kMaxBlocks);
+int64_t partial_slots(const FineOperator&) { return kMaxBlocks; }
+
+template <int DIM>
+Seg fine_seg(const FineOperator& op) {
+  return make_seg<DIM>(op.A.nx, op.A.ny, op.A.nz);
+}
+
+void launch_init(LearnedSolver* s, const FineOperator& op, Loop h, cudaStream_t st) {
+  if (op.dim == 2) {
+    const Seg sg = fine_seg<2>(op);
+    k_fcg_init<2><<<seg_grid(sg), kT, 0, st>>>(op.A, sg, s->S, s->r, s->r32, s->partials, s->hist,
+                                               s->hist_cap, h);
+  } else {
+    const Seg sg = fine_seg<3>(op);
+    k_fcg_init<3><<<seg_grid(sg), kT, 0, st>>>(op.A, sg, s->S, s->r, s->r32, s->partials, s->hist,
+                                               s->hist_cap, h);
+  }
 }
 
 // One FCG iteration: V-cycle z = M r (its last kernel also forms z.q and
 // beta), direction + A p, update.  Returns the number of kernels.
 int enqueue_body(LearnedSolver* s, const FineOperator& op, Loop h, cudaStream_t st) {
   const int64_t skip = op.pinned ? op.ref : -1;
-  const Shape sh = cells_shape(op.A.nx, (int64_t)op.A.ny * op.A.nz);
   const Hook hk{s->q, s->partials, s->S, h};
-  const int nv = op.dim == 2 ? enqueue_cycle<2>(*s->H, s->W, s->r32, s->z32, skip, &hk, st)
-                             : enqueue_cycle<3>(*s->H, s->W, s->r32, s->z32, skip, &hk, st);
-  k_fcg_dir<<<sh.grid, sh.block, 0, st>>>(op.A, s->S, s->z32, s->p0, s->p1, s->q, s->r,
-                                           s->partials, h);
+  int nv;
+  if (op.dim == 2) {
+    nv = enqueue_cycle<2>(*s->H, s->W, s->r32, s->z32, skip, &hk, st);
+    const Seg sg = fine_seg<2>(op);
+    k_fcg_dir<2><<<seg_grid(sg), kT, 0, st>>>(op.A, sg, s->S, s->z32, s->p0, s->p1, s->q, s->r,
+                                              s->partials, h);
+  } else {
+    nv = enqueue_cycle<3>(*s->H, s->W, s->r32, s->z32, skip, &hk, st);
+    const Seg sg = fine_seg<3>(op);
+    k_fcg_dir<3><<<seg_grid(sg), kT, 0, st>>>(op.A, sg, s->S, s->z32, s->p0, s->p1, s->q, s->r,
+                                              s->partials, h);
+  }
   k_fcg_update<<<flat_grid(s->cells), 256, 0, st>>>(s->cells, s->S, s->r, s->r32, s->p0, s->p1,
                                                     s->q, s->partials, s->hist, s->hist_cap, h);
   return nv + 2;
@@ -959,9 +1145,7 @@ int enqueue_body(LearnedSolver* s, const FineOperator& op, Loop h, cudaStream_t 
 // with conditional nodes (CFDB_LEARNED_LAUNCH=stream): the same kernels,
 // launched per iteration, the host reading the state after each iteration.
 cfdb_status run_stream_mode(cfdb_context* ctx, LearnedSolver* s, const FineOperator& op) {
-  const Shape sh = cells_shape(op.A.nx, (int64_t)op.A.ny * op.A.nz);
-  k_fcg_init<<<sh.grid, sh.block, 0, ctx->stream>>>(op.A, s->S, s->r, s->r32, s->partials, s->hist,
-                                                     s->hist_cap, Loop{0, 0});
+  launch_init(s, op, Loop{0, 0}, ctx->stream);
   CFDB_CHECK_LAUNCH(ctx);
   while (true) {
     CFDB_CUDA(ctx, cudaMemcpyAsync(s->S_host, s->S, sizeof(FcgState), cudaMemcpyDeviceToHost,
@@ -979,13 +1163,11 @@ cfdb_status capture_graph(cfdb_context* ctx, LearnedSolver* s, const FineOperato
   CFDB_CUDA(ctx, cudaGraphCreate(&s->graph, 0));
   cudaGraphConditionalHandle h;
   CFDB_CUDA(ctx, cudaGraphConditionalHandleCreate(&h, s->graph, 1, cudaGraphCondAssignDefault));
-  const Shape sh = cells_shape(op.A.nx, (int64_t)op.A.ny * op.A.nz);
   // parent graph: the initial residual, then the WHILE node
   CFDB_CUDA(ctx, cudaStreamBeginCaptureToGraph(s->cap, s->graph, nullptr, nullptr, 0,
                                                cudaStreamCaptureModeThreadLocal));
   const Loop lp{h, 1};
-  k_fcg_init<<<sh.grid, sh.block, 0, s->cap>>>(op.A, s->S, s->r, s->r32, s->partials, s->hist,
-                                                s->hist_cap, lp);
+  launch_init(s, op, lp, s->cap);
   cudaGraph_t g = nullptr;
   cudaError_t ce = cudaStreamEndCapture(s->cap, &g);
   if (ce != cudaSuccess) return cuda_error(ctx, ce, "capture of the FCG start", __FILE__, __LINE__);
@@ -1016,7 +1198,7 @@ cfdb_status capture_graph(cfdb_context* ctx, LearnedSolver* s, const FineOperato
   // V-cycle, the direction pass (z, p_old, r in; p, q out), the update (x, p,
   // r, q in; x, r, r32 out) and the z.q read of q; face arrays when present
   int face_words = 0;
-  for (int a = 0; a < op.dim; ++a) face_words += op.full[a] ? 1 : 0;
+  for (int a = 0; a < 3; ++a) face_words += op.full[a] ? 1 : 0;
   const double n = (double)s->cells;
   s->bytes_init = n * (8.0 * (3 + face_words) + 4.0);
   s->bytes_iter = cycle_bytes(*s->H, s->W) + n * (4.0 + 8.0 * (4 + face_words)) +
@@ -1031,7 +1213,7 @@ cfdb_status learned_solve(cfdb_context* ctx, LearnedSolver* s, const FineOperato
                           double abs_tol, double rel_tol, int64_t max_it, int64_t hist_cap,
                           LearnedOutcome* out) {
   std::memset(out, 0, sizeof(*out));
-  const int64_t cells = (int64_t)op.n[0] * op.n[1] * (op.dim == 3 ? op.n[2] : 1);
+  const int64_t cells = (int64_t)op.n[0] * op.n[1] * op.n[2];
   const bool same_shape = s->H && s->dim == op.dim && s->n[0] == op.n[0] && s->n[1] == op.n[1] &&
                           s->n[2] == op.n[2];
   bool recapture = false;

@@ -48,10 +48,12 @@ MgWeights mg_default_weights(int dim);
 // Checks the symmetry and finiteness a usable weight set needs.
 bool mg_weights_valid(const MgWeights& W, std::string* why);
 
+// Levels live in kernel space: a 2D grid (nx, ny) is (nx, 1, ny) with no
+// y-faces, so one set of kernels serves the 5- and 7-point operators.
 struct MgLevel {
-  int n[3];  // cells per axis (n[2] = 1 in 2D)
+  int n[3];  // kernel-space cells per axis
   int64_t cells;
-  float* f[3];  // face coefficients per axis, global per-axis face layout
+  float* f[3];  // face coefficients per kernel axis (f[1] null in 2D)
   float* isq;   // D^-1/2 (0 where the diagonal is 0)
   float* x;     // correction of this level
   float* r;     // right-hand side of this level
@@ -71,15 +73,16 @@ struct MgHierarchy {
   ~MgHierarchy();
 };
 
-// The fine operator as the learned solve sees it: kernel-space FP64 view
-// (the exact reference operator, pinned row included) and, per real axis,
-// either a full face array or a per-axis table of face coefficients.
+// The fine operator as the learned solve sees it, in kernel space: the FP64
+// view (the exact reference operator, pinned row included) and, per kernel
+// axis, either a full face array or a per-axis table of face coefficients
+// (both null for the 2D y axis).
 struct FineOperator {
   int dim;
-  int n[3];                // real cells per axis (n[2] = 1 in 2D)
-  OpView<double> A;        // kernel space (2D: nx x 1 x ny)
-  const double* full[3];   // per real axis: global face array, or null
-  const double* table[3];  // per real axis: coefficient by face coordinate
+  int n[3];                // kernel-space cells per axis
+  OpView<double> A;
+  const double* full[3];
+  const double* table[3];
   int pinned;
   int64_t ref;
 };

@@ -744,14 +744,14 @@ cfdb_status solve_learned(cfdb_context* ctx, cfdb_poperator* op, const cfdb_line
   FineOperator fo;
   std::memset(&fo, 0, sizeof(fo));
   fo.dim = g.dim;
-  fo.n[0] = (int)g.n[0];
-  fo.n[1] = (int)g.n[1];
-  fo.n[2] = g.dim == 3 ? (int)g.n[2] : 1;
+  fo.n[0] = op->knx;
+  fo.n[1] = op->kny;
+  fo.n[2] = op->knz;
   fo.A = view<double>(op);
-  const int kaxis[3] = {0, g.dim == 2 ? 2 : 1, 2};
-  for (int a = 0; a < g.dim; ++a) {
-    fo.full[a] = op->f64[kaxis[a]];
-    fo.table[a] = op->t64[kaxis[a]];
+  for (int q = 0; q < 3; ++q) {
+    const bool active = g.dim == 3 || q != 1;  // 2D kernel space has no y-faces
+    fo.full[q] = active ? op->f64[q] : nullptr;
+    fo.table[q] = active ? op->t64[q] : nullptr;
   }
   fo.pinned = op->pinned;
   fo.ref = op->ref;
