@@ -107,6 +107,9 @@ def load() -> C.CDLL:
     L.cfdb_mg_set_weights.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, fp, fp]
     L.cfdb_mg_get_weights.argtypes = [vp, C.c_int, ip, ip, ip, fp, fp]
     L.cfdb_mg_reset_weights.argtypes = [vp, C.c_int, C.c_int]
+    L.cfdb_mg_apply.argtypes = [vp, vp, fp, fp]
+    L.cfdb_mg_loss_grad.argtypes = [vp, vp, C.c_int, fp, C.POINTER(dbl), C.POINTER(dbl),
+                                    C.POINTER(dbl)]
     _lib = L
     return L
 
@@ -365,6 +368,27 @@ class POperator:
             _dp(hist) if history_cap > 0 else None, history_cap, C.byref(res)),
             "cfdb_poperator_solve_device")
         return self._result(res, hist, history_cap)
+
+    # learned preconditioner (cfdb_mg_*)
+    def mg_apply(self, r: np.ndarray) -> np.ndarray:
+        """z = M r through the solve's V-cycle kernels (FP32)."""
+        rr = np.ascontiguousarray(r, dtype=np.float32).reshape(-1)
+        z = np.empty_like(rr)
+        fp = C.POINTER(C.c_float)
+        self.ctx.check(self.ctx.lib.cfdb_mg_apply(self.ctx.handle, self._h, rr.ctypes.data_as(fp),
+                                                  z.ctypes.data_as(fp)), "cfdb_mg_apply")
+        return z
+
+    def mg_loss_grad(self, e: np.ndarray):
+        """Loss and gradient of the context's network on error fields e (samples x cells)."""
+        ee = np.ascontiguousarray(e, dtype=np.float32).reshape(-1, self.cells)
+        loss = C.c_double()
+        gk = np.zeros((MG_MAX_LEVELS, MG_TAPS))
+        gc = np.zeros(MG_MAX_LEVELS)
+        self.ctx.check(self.ctx.lib.cfdb_mg_loss_grad(
+            self.ctx.handle, self._h, len(ee), ee.ctypes.data_as(C.POINTER(C.c_float)),
+            C.byref(loss), _dp(gk), _dp(gc)), "cfdb_mg_loss_grad")
+        return loss.value, gk, gc
 
     def close(self):
         if getattr(self, "_h", None):

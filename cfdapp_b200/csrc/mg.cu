@@ -33,6 +33,7 @@
 #include "cfdb_internal.cuh"
 #include "grid_sync.cuh"
 #include "mg.cuh"
+#include "pcg_internal.cuh"
 
 namespace cfdb {
 
@@ -87,15 +88,23 @@ constexpr int kMaxCoarse = 8;
 constexpr int kCoarseThreads = 1024;
 constexpr size_t kCoarseSmemCap = 200 * 1024;
 
+// Thread layout of the tiled kernels: TX x TY threads, each owning CX cells
+// of a plane row strided by TX (so every load instruction is coalesced).
 template <int DIM>
 struct Tile;
+// Shared-memory rows of a plane buffer: the TY rows plus a y-halo row on
+// each side when TY > 1 (a 2D row has no y-neighbours).
+template <int TY>
+struct Rows {
+  static constexpr int R0 = TY > 1 ? 1 : 0, N = TY + 2 * R0;
+};
 template <>
 struct Tile<2> {
-  static constexpr int PX = 256, PY = 1;
+  static constexpr int TX = 256, TY = 1;
 };
 template <>
 struct Tile<3> {
-  static constexpr int PX = 32, PY = 8;
+  static constexpr int TX = 32, TY = 8;
 };
 
 struct Kern {
@@ -129,6 +138,15 @@ Kern kern_of(const MgWeights& W, int l) {
   return K;
 }
 float cw_of(const MgWeights& W, int l) { return W.c[std::min(l, W.levels - 1)]; }
+
+}  // namespace
+
+void mg_kernel_taps(const MgWeights& W, int l, float out[kMgTaps]) {
+  const Kern K = kern_of(W, l);
+  std::memcpy(out, K.w, sizeof(K.w));
+}
+
+namespace {
 
 __device__ __forceinline__ int64_t at(const LV& L, int i, int j, int k) {
   return i + (int64_t)L.nx * (j + (int64_t)L.ny * k);
@@ -180,17 +198,30 @@ struct Seg {
   int64_t items;
 };
 
-template <int DIM>
+template <int DIM, int CX>
 Seg make_seg(int nx, int ny, int nz) {
+  constexpr int PX = Tile<DIM>::TX * CX, PY = Tile<DIM>::TY;
   Seg s;
-  s.tiles_x = (nx + Tile<DIM>::PX - 1) / Tile<DIM>::PX;
-  const int64_t tiles = (int64_t)s.tiles_x * ((ny + Tile<DIM>::PY - 1) / Tile<DIM>::PY);
+  s.tiles_x = (nx + PX - 1) / PX;
+  const int64_t tiles = (int64_t)s.tiles_x * ((ny + PY - 1) / PY);
   s.pairs = (nz + 1) / 2;
   s.items = tiles * s.pairs;
   return s;
 }
 
-int seg_grid(const Seg& s) { return (int)std::max<int64_t>(1, std::min<int64_t>(s.items, kGridCap)); }
+// Blocks for a pass: at most kGridCap, each with the same number of items.
+int seg_grid(const Seg& s) {
+  const int64_t per = std::max<int64_t>(1, (s.items + kGridCap - 1) / kGridCap);
+  return (int)std::max<int64_t>(1, (s.items + per - 1) / per);
+}
+
+// Four cells per thread where the level is wide enough.
+// (2D rows stay at one cell per thread: with only nx/1024 tiles per row the
+// plane runs get too short to hide the z-halo reloads.)
+template <int DIM>
+bool wide(int nx) {
+  return DIM == 3 && nx >= Tile<DIM>::TX * 4;
+}
 
 // f(tix, tiy, k0, k1) for every plane run of this block.
 template <class F>
@@ -207,87 +238,129 @@ __device__ __forceinline__ void for_runs(const Seg& sg, int nz, F f) {
   }
 }
 
-// 7-point march: val(i,j,k) is the stencil input; cell(act, i, j, k, v, w, e,
-// s, n, b, t) runs in EVERY thread for every plane (act: the thread owns an
-// in-domain cell), so it may use warp and block collectives.
-template <typename T, int PX, int PY, class Val, class Cell>
+// 7-point march over planes [k0, k1) of tile (tix, tiy): val(i,j,k) is the
+// stencil input.  For every plane, cell(c, act, i, j, k, v, w, e, s, n, b, t)
+// runs for each of the thread's CX cells, then after(k) runs once in EVERY
+// thread (it may use warp and block collectives).  z-neighbours stay in
+// registers; the plane with its x/y halo is staged in shared memory.
+template <typename T, int TX, int TY, int CX, class Val, class Cell, class After>
 __device__ __forceinline__ void march7(int nx, int ny, int nz, int tix, int tiy, int k0, int k1,
-                                       T (*buf)[PY + 2][PX + 2], Val val, Cell cell) {
-  const int tx = threadIdx.x % PX, ty = threadIdx.x / PX;
-  const int i = tix * PX + tx, j = tiy * PY + ty;
-  const bool act = i < nx && j < ny;
-  T vprev = T(0), vcur = T(0);
-  if (act) {
-    if (k0 > 0) vprev = val(i, j, k0 - 1);
-    vcur = val(i, j, k0);
+                                       T (*buf)[Rows<TY>::N][TX * CX + 2], Val val, Cell cell,
+                                       After after) {
+  constexpr int PX = TX * CX, R0 = Rows<TY>::R0;
+  const int tx = threadIdx.x % TX, ty = threadIdx.x / TX;
+  const int x0 = tix * PX, j = tiy * TY + ty;
+  const bool row = j < ny;
+  T vp[CX], vc[CX], vn[CX];
+#pragma unroll
+  for (int c = 0; c < CX; ++c) {
+    const int i = x0 + tx + c * TX;
+    const bool a = row && i < nx;
+    vp[c] = (a && k0 > 0) ? val(i, j, k0 - 1) : T(0);
+    vc[c] = a ? val(i, j, k0) : T(0);
   }
   for (int k = k0; k < k1; ++k) {
-    const T vnext = (act && k + 1 < nz) ? val(i, j, k + 1) : T(0);
     T(*s)[PX + 2] = buf[k & 1];
-    s[ty + 1][tx + 1] = vcur;
-    if (tx == 0) s[ty + 1][0] = (i > 0 && j < ny) ? val(i - 1, j, k) : T(0);
-    if (tx == PX - 1) s[ty + 1][PX + 1] = (i + 1 < nx && j < ny) ? val(i + 1, j, k) : T(0);
-    if (PY > 1) {
-      if (ty == 0) s[0][tx + 1] = (j > 0 && i < nx) ? val(i, j - 1, k) : T(0);
-      if (ty == PY - 1) s[PY + 1][tx + 1] = (j + 1 < ny && i < nx) ? val(i, j + 1, k) : T(0);
+#pragma unroll
+    for (int c = 0; c < CX; ++c) {
+      const int i = x0 + tx + c * TX;
+      vn[c] = (row && i < nx && k + 1 < nz) ? val(i, j, k + 1) : T(0);
+      s[ty + R0][1 + tx + c * TX] = vc[c];
+    }
+    if (tx == 0) s[ty + R0][0] = (row && x0 > 0) ? val(x0 - 1, j, k) : T(0);
+    if (tx == TX - 1) s[ty + R0][PX + 1] = (row && x0 + PX < nx) ? val(x0 + PX, j, k) : T(0);
+    if (TY > 1) {
+      if (ty == 0) {
+#pragma unroll
+        for (int c = 0; c < CX; ++c) {
+          const int i = x0 + tx + c * TX;
+          s[0][1 + tx + c * TX] = (j > 0 && i < nx) ? val(i, j - 1, k) : T(0);
+        }
+      }
+      if (ty == TY - 1) {
+#pragma unroll
+        for (int c = 0; c < CX; ++c) {
+          const int i = x0 + tx + c * TX;
+          s[TY + 1][1 + tx + c * TX] = (j + 1 < ny && i < nx) ? val(i, j + 1, k) : T(0);
+        }
+      }
     }
     __syncthreads();
-    const T vs = (PY > 1) ? s[ty][tx + 1] : T(0);
-    const T vn = (PY > 1) ? s[ty + 2][tx + 1] : T(0);
-    cell(act, i, j, k, vcur, s[ty + 1][tx], s[ty + 1][tx + 2], vs, vn, vprev, vnext);
-    vprev = vcur;
-    vcur = vnext;
+#pragma unroll
+    for (int c = 0; c < CX; ++c) {
+      const int xi = 1 + tx + c * TX;
+      const int i = x0 + tx + c * TX;
+      const T vs = (TY > 1) ? s[ty][xi] : T(0);
+      const T vnn = (TY > 1) ? s[ty + 2][xi] : T(0);
+      cell(c, row && i < nx, i, j, k, vc[c], s[ty + R0][xi - 1], s[ty + R0][xi + 1], vs, vnn, vp[c],
+           vn[c]);
+    }
+    after(k);
+#pragma unroll
+    for (int c = 0; c < CX; ++c) {
+      vp[c] = vc[c];
+      vc[c] = vn[c];
+    }
   }
   __syncthreads();
 }
 
-// 27-point (2D: 9-point) convolution march over a three-plane ring:
-// u(i,j,k) is the convolved field, cell(act, i, j, k, sum) runs in every
-// thread for every plane with sum = sum_o K[o] u(c+o) (0 outside the domain).
-template <int PX, int PY, bool TWO_D, class U, class Cell>
+// 27-point (2D: 9-point) convolution march over a three-plane ring: u(i,j,k)
+// is the convolved field; cell(c, act, i, j, k, sum) runs for each of the
+// thread's CX cells of every plane with sum = sum_o K[o] u(cell+o) (0 outside
+// the domain).
+template <int TX, int TY, int CX, bool TWO_D, class U, class Cell>
 __device__ __forceinline__ void march27(int nx, int ny, int nz, int tix, int tiy, int k0, int k1,
-                                        float (*ring)[PY + 2][PX + 2], const Kern& K, U u,
-                                        Cell cell) {
+                                        float (*ring)[Rows<TY>::N][TX * CX + 2], const Kern& K,
+                                        U u, Cell cell) {
+  constexpr int PX = TX * CX, R0 = Rows<TY>::R0;
+  static_assert(!TWO_D || TY == 1, "a 2D plane is one row");
   const int tid = threadIdx.x;
-  const int tx = tid % PX, ty = tid / PX;
-  const int i = tix * PX + tx, j = tiy * PY + ty;
-  const bool act = i < nx && j < ny;
-  auto load = [&](int kp) {
-    float(*s)[PX + 2] = ring[(kp + 3) % 3];
+  const int tx = tid % TX, ty = tid / TX;
+  const int x0 = tix * PX, j = tiy * TY + ty;
+  auto load = [&](int kp, int slot) {
+    float(*s)[PX + 2] = ring[slot];
+    const bool zin = kp >= 0 && kp < nz;
     if (TWO_D) {
-      for (int q = tid; q < PX + 2; q += PX * PY) {
-        const int gi = tix * PX + q - 1;
-        s[1][q] = (kp >= 0 && kp < nz && gi >= 0 && gi < nx) ? u(gi, 0, kp) : 0.f;
+      for (int q = tid; q < PX + 2; q += TX * TY) {
+        const int gi = x0 + q - 1;
+        s[0][q] = (zin && gi >= 0 && gi < nx) ? u(gi, 0, kp) : 0.f;
       }
     } else {
-      for (int q = tid; q < (PY + 2) * (PX + 2); q += PX * PY) {
+      for (int q = tid; q < (TY + 2) * (PX + 2); q += TX * TY) {
         const int hy = q / (PX + 2), hx = q % (PX + 2);
-        const int gi = tix * PX + hx - 1, gj = tiy * PY + hy - 1;
-        s[hy][hx] = (kp >= 0 && kp < nz && gi >= 0 && gi < nx && gj >= 0 && gj < ny)
-                        ? u(gi, gj, kp)
-                        : 0.f;
+        const int gi = x0 + hx - 1, gj = tiy * TY + hy - 1;
+        s[hy][hx] = (zin && gi >= 0 && gi < nx && gj >= 0 && gj < ny) ? u(gi, gj, kp) : 0.f;
       }
     }
   };
-  load(k0 - 1);
-  load(k0);
+  // slots rotate: lo holds plane k-1, mi plane k, hi plane k+1
+  int lo = 0, mi = 1, hi = 2;
+  load(k0 - 1, lo);
+  load(k0, mi);
   for (int k = k0; k < k1; ++k) {
-    load(k + 1);
+    load(k + 1, hi);
     __syncthreads();
-    float sum = 0.f;
-    if (act) {
+    const float(*pl[3])[PX + 2] = {ring[lo], ring[mi], ring[hi]};  // planes k-1, k, k+1
 #pragma unroll
-      for (int dk = -1; dk <= 1; ++dk) {
-        const float(*s)[PX + 2] = ring[(k + dk + 3) % 3];
+    for (int c = 0; c < CX; ++c) {
+      const int xi = 1 + tx + c * TX;
+      float sum = 0.f;
+#pragma unroll
+      for (int dk = 0; dk < 3; ++dk)
 #pragma unroll
         for (int dj = (TWO_D ? 0 : -1); dj <= (TWO_D ? 0 : 1); ++dj)
 #pragma unroll
           for (int di = -1; di <= 1; ++di)
-            sum += K.w[(dk + 1) * 9 + (dj + 1) * 3 + (di + 1)] * s[ty + 1 + dj][tx + 1 + di];
-      }
+            sum += K.w[dk * 9 + (dj + 1) * 3 + (di + 1)] * pl[dk][ty + R0 + dj][xi + di];
+      const int i = x0 + tx + c * TX;
+      cell(c, j < ny && i < nx, i, j, k, sum);
     }
-    cell(act, i, j, k, sum);
     __syncthreads();
+    const int t = lo;
+    lo = mi;
+    mi = hi;
+    hi = t;
   }
 }
 
@@ -365,45 +438,58 @@ struct Hook {
 
 // res = r - A x  (PRO: x + cw P ec in place of x).  RESTRICT: instead of
 // storing res, rc(parent) = sum of the children's res.  r[skip] reads as 0.
-template <int DIM, bool PRO, bool RESTRICT>
+template <int DIM, int CX, bool PRO, bool RESTRICT>
 __global__ void __launch_bounds__(kT) k_res(LV L, LV C, Seg sg, const float* __restrict__ x,
                                             const float* __restrict__ ec, float cw,
                                             const float* __restrict__ r, float* __restrict__ res,
                                             float* __restrict__ rc, int64_t skip) {
-  constexpr int PX = Tile<DIM>::PX, PY = Tile<DIM>::PY;
-  __shared__ float buf[2][PY + 2][PX + 2];
-  __shared__ float rows[PY][PX / 2];
-  const int tx = threadIdx.x % PX, ty = threadIdx.x / PX;
+  constexpr int TX = Tile<DIM>::TX, TY = Tile<DIM>::TY, PX = TX * CX;
+  __shared__ float buf[2][Rows<TY>::N][PX + 2];
+  __shared__ float rows[TY][CX][TX / 2];
+  const int tx = threadIdx.x % TX, ty = threadIdx.x / TX;
   auto val = [&](int i, int j, int k) {
     float v = x[at(L, i, j, k)];
     if (PRO) v += cw * ec[parent(C, i, j, k)];
     return v;
   };
   for_runs(sg, L.nz, [&](int tix, int tiy, int k0, int k1) {
-    float racc = 0.f;
-    march7<float, PX, PY>(
+    float rv[CX], racc[CX];
+#pragma unroll
+    for (int c = 0; c < CX; ++c) racc[c] = 0.f;
+    const int x0 = tix * PX, j = tiy * TY + ty;
+    march7<float, TX, TY, CX>(
         L.nx, L.ny, L.nz, tix, tiy, k0, k1, buf, val,
-        [&](bool act, int i, int j, int k, float v, float w, float e, float s, float n, float b,
-            float t) {
-          float rv = 0.f;
+        [&](int c, bool act, int i, int jj, int k, float v, float w, float e, float s, float n,
+            float b, float t) {
+          rv[c] = 0.f;
           if (act) {
-            const int64_t c = at(L, i, j, k);
-            rv = (c == skip ? 0.f : r[c]) - apply7(coef<DIM>(L, i, j, k), v, w, e, s, n, b, t);
-            if (!RESTRICT) res[c] = rv;
+            const int64_t q = at(L, i, jj, k);
+            rv[c] = (q == skip ? 0.f : r[q]) - apply7(coef<DIM>(L, i, jj, k), v, w, e, s, n, b, t);
+            if (!RESTRICT) res[q] = rv[c];
           }
-          if (RESTRICT) {
-            const float xs = rv + __shfl_xor_sync(0xffffffffu, rv, 1);
-            float quad = xs;
-            if (PY > 1) {
-              if ((tx & 1) == 0) rows[ty][tx >> 1] = xs;
-              __syncthreads();
-              if ((tx & 1) == 0 && (ty & 1) == 0) quad = xs + rows[ty + 1][tx >> 1];
-            }
-            racc = ((k & 1) == 0) ? quad : racc + quad;
-            const bool writer = (tx & 1) == 0 && (PY == 1 || (ty & 1) == 0);
-            if (writer && ((k & 1) == 1 || k + 1 == L.nz)) {
-              const int ci = i >> 1, cj = j >> 1, ck = k >> 1;
-              if (ci < C.nx && cj < C.ny) rc[ci + (int64_t)C.nx * (cj + (int64_t)C.ny * ck)] = racc;
+        },
+        [&](int k) {
+          if constexpr (!RESTRICT) return;
+          float quad[CX];
+#pragma unroll
+          for (int c = 0; c < CX; ++c) quad[c] = rv[c] + __shfl_xor_sync(0xffffffffu, rv[c], 1);
+          if (TY > 1) {
+            if ((tx & 1) == 0)
+#pragma unroll
+              for (int c = 0; c < CX; ++c) rows[ty][c][tx >> 1] = quad[c];
+            __syncthreads();
+            if ((tx & 1) == 0 && (ty & 1) == 0)
+#pragma unroll
+              for (int c = 0; c < CX; ++c) quad[c] += rows[ty + 1][c][tx >> 1];
+          }
+          const bool writer = (tx & 1) == 0 && (TY == 1 || (ty & 1) == 0);
+          const bool flush = (k & 1) == 1 || k + 1 == L.nz;
+#pragma unroll
+          for (int c = 0; c < CX; ++c) {
+            racc[c] = ((k & 1) == 0) ? quad[c] : racc[c] + quad[c];
+            if (writer && flush) {
+              const int ci = (x0 + tx + c * TX) >> 1, cj = j >> 1, ck = k >> 1;
+              if (ci < C.nx && cj < C.ny) rc[ci + (int64_t)C.nx * (cj + (int64_t)C.ny * ck)] = racc[c];
             }
           }
         });
@@ -415,13 +501,13 @@ enum { SM_FIRST = 0, SM_ADD = 1 };
 // x <- [x] (+ cw P ec) + D^-1/2 (W * (D^-1/2 u)), u = res (SM_ADD) or r with
 // r[skip] = 0 and x = 0 before (SM_FIRST).  pin >= 0: z[pin] = r[pin] (the
 // last sweep of level 0); HOOK: also accumulate z.q for the FCG coefficient.
-template <int DIM, int MODE, bool HOOK>
+template <int DIM, int CX, int MODE, bool HOOK>
 __global__ void __launch_bounds__(kT) k_sm(LV L, LV C, Seg sg, Kern K, const float* __restrict__ src,
                                            const float* __restrict__ ec, float cw,
                                            float* __restrict__ x, int64_t skip, int64_t pin,
                                            const float* __restrict__ r, Hook hk) {
-  constexpr int PX = Tile<DIM>::PX, PY = Tile<DIM>::PY;
-  __shared__ float ring[3][PY + 2][PX + 2];
+  constexpr int TX = Tile<DIM>::TX, TY = Tile<DIM>::TY, PX = TX * CX;
+  __shared__ float ring[3][Rows<TY>::N][PX + 2];
   double acc[1] = {0.0};
   auto u = [&](int i, int j, int k) {
     const int64_t q = at(L, i, j, k);
@@ -429,17 +515,17 @@ __global__ void __launch_bounds__(kT) k_sm(LV L, LV C, Seg sg, Kern K, const flo
     return src[q] * L.isq[q];
   };
   for_runs(sg, L.nz, [&](int tix, int tiy, int k0, int k1) {
-    march27<PX, PY, DIM == 2>(L.nx, L.ny, L.nz, tix, tiy, k0, k1, ring, K, u,
-                              [&](bool act, int i, int j, int k, float sum) {
-                                if (!act) return;
-                                const int64_t c = at(L, i, j, k);
-                                float v = L.isq[c] * sum;
-                                if (MODE == SM_ADD) v += x[c];
-                                if (ec) v += cw * ec[parent(C, i, j, k)];
-                                if (c == pin) v = r[c];
-                                x[c] = v;
-                                if (HOOK) acc[0] += (double)v * hk.q[c];
-                              });
+    march27<TX, TY, CX, DIM == 2>(L.nx, L.ny, L.nz, tix, tiy, k0, k1, ring, K, u,
+                                  [&](int, bool act, int i, int j, int k, float sum) {
+                                    if (!act) return;
+                                    const int64_t c = at(L, i, j, k);
+                                    float v = L.isq[c] * sum;
+                                    if (MODE == SM_ADD) v += x[c];
+                                    if (ec) v += cw * ec[parent(C, i, j, k)];
+                                    if (c == pin) v = r[c];
+                                    x[c] = v;
+                                    if (HOOK) acc[0] += (double)v * hk.q[c];
+                                  });
   });
   if (HOOK) {
     reduce_last<1>(acc, hk.partials, &hk.S->ticket, [&](const double* tot) {
@@ -746,6 +832,50 @@ CoarsePlan coarse_plan(const MgHierarchy& H, const MgWeights& W) {
   return P;
 }
 
+// Launchers of one level's passes, with the cells-per-thread choice.
+template <int DIM, int CX>
+struct LevelOps {
+  static void res(const MgLevel& M, const LV& LC, const float* x, const float* ec, float cw,
+                  const float* r, float* res, float* rc, int64_t skip, cudaStream_t st) {
+    const Seg sg = make_seg<DIM, CX>(M.n[0], M.n[1], M.n[2]);
+    const LV L = lv(M);
+    if (rc)
+      k_res<DIM, CX, false, true><<<seg_grid(sg), kT, 0, st>>>(L, LC, sg, x, ec, cw, r, res, rc, skip);
+    else if (ec)
+      k_res<DIM, CX, true, false><<<seg_grid(sg), kT, 0, st>>>(L, LC, sg, x, ec, cw, r, res, rc, skip);
+    else
+      k_res<DIM, CX, false, false><<<seg_grid(sg), kT, 0, st>>>(L, LC, sg, x, ec, cw, r, res, rc, skip);
+  }
+  static void sm(const MgLevel& M, const LV& LC, const Kern& K, bool first, const float* src,
+                 const float* ec, float cw, float* x, int64_t skip, int64_t pin, const float* r,
+                 const Hook* hook, cudaStream_t st) {
+    const Seg sg = make_seg<DIM, CX>(M.n[0], M.n[1], M.n[2]);
+    const LV L = lv(M);
+    const int g = seg_grid(sg);
+    if (first)
+      k_sm<DIM, CX, SM_FIRST, false><<<g, kT, 0, st>>>(L, LC, sg, K, src, ec, cw, x, skip, pin, r, Hook{});
+    else if (hook)
+      k_sm<DIM, CX, SM_ADD, true><<<g, kT, 0, st>>>(L, LC, sg, K, src, ec, cw, x, skip, pin, r, *hook);
+    else
+      k_sm<DIM, CX, SM_ADD, false><<<g, kT, 0, st>>>(L, LC, sg, K, src, ec, cw, x, skip, pin, r, Hook{});
+  }
+};
+
+template <int DIM>
+void level_res(const MgLevel& M, const LV& LC, const float* x, const float* ec, float cw,
+               const float* r, float* res, float* rc, int64_t skip, cudaStream_t st) {
+  if (wide<DIM>(M.n[0])) LevelOps<DIM, 4>::res(M, LC, x, ec, cw, r, res, rc, skip, st);
+  else LevelOps<DIM, 1>::res(M, LC, x, ec, cw, r, res, rc, skip, st);
+}
+
+template <int DIM>
+void level_sm(const MgLevel& M, const LV& LC, const Kern& K, bool first, const float* src,
+              const float* ec, float cw, float* x, int64_t skip, int64_t pin, const float* r,
+              const Hook* hook, cudaStream_t st) {
+  if (wide<DIM>(M.n[0])) LevelOps<DIM, 4>::sm(M, LC, K, first, src, ec, cw, x, skip, pin, r, hook, st);
+  else LevelOps<DIM, 1>::sm(M, LC, K, first, src, ec, cw, x, skip, pin, r, hook, st);
+}
+
 // Enqueues z = M r (level-0 FP32 vectors) on `st`; returns the number of
 // kernels launched.
 template <int DIM>
@@ -757,23 +887,17 @@ int enqueue_cycle(const MgHierarchy& H, const MgWeights& W, const float* r0, flo
   auto xp = [&](int l) -> float* { return l == 0 ? z0 : H.L[l].x; };
   for (int l = 0; l < cf; ++l) {
     const MgLevel& M = H.L[l];
-    const LV L = lv(M), LC = lv(H.L[l + 1]);
+    const LV LC = lv(H.L[l + 1]);
     const Kern K = kern_of(W, l);
     const int64_t sk = l == 0 ? skip : -1;
-    const Seg sg = make_seg<DIM>(M.n[0], M.n[1], M.n[2]);
-    const int g = seg_grid(sg);
-    k_sm<DIM, SM_FIRST, false><<<g, kT, 0, st>>>(L, LC, sg, K, rp(l), nullptr, 0.f, xp(l), sk, -1,
-                                                 nullptr, Hook{});
+    level_sm<DIM>(M, LC, K, true, rp(l), nullptr, 0.f, xp(l), sk, -1, nullptr, nullptr, st);
     ++launches;
     for (int q = 1; q < W.nu; ++q) {
-      k_res<DIM, false, false><<<g, kT, 0, st>>>(L, LC, sg, xp(l), nullptr, 0.f, rp(l), M.res,
-                                                 nullptr, sk);
-      k_sm<DIM, SM_ADD, false><<<g, kT, 0, st>>>(L, LC, sg, K, M.res, nullptr, 0.f, xp(l), -1, -1,
-                                                 nullptr, Hook{});
+      level_res<DIM>(M, LC, xp(l), nullptr, 0.f, rp(l), M.res, nullptr, sk, st);
+      level_sm<DIM>(M, LC, K, false, M.res, nullptr, 0.f, xp(l), -1, -1, nullptr, nullptr, st);
       launches += 2;
     }
-    k_res<DIM, false, true><<<g, kT, 0, st>>>(L, LC, sg, xp(l), nullptr, 0.f, rp(l), nullptr,
-                                              H.L[l + 1].r, sk);
+    level_res<DIM>(M, LC, xp(l), nullptr, 0.f, rp(l), nullptr, H.L[l + 1].r, sk, st);
     ++launches;
   }
   if (cf < H.levels) {
@@ -784,27 +908,16 @@ int enqueue_cycle(const MgHierarchy& H, const MgWeights& W, const float* r0, flo
   for (int l = cf - 1; l >= 0; --l) {
     const MgLevel& M = H.L[l];
     const MgLevel& C = H.L[l + 1];
-    const LV L = lv(M), LC = lv(C);
+    const LV LC = lv(C);
     const Kern K = kern_of(W, l);
     const float cw = cw_of(W, l);
     const int64_t sk = l == 0 ? skip : -1;
-    const Seg sg = make_seg<DIM>(M.n[0], M.n[1], M.n[2]);
-    const int g = seg_grid(sg);
     for (int q = 0; q < W.nu; ++q) {
       const float* ec = q == 0 ? C.x : nullptr;
-      if (q == 0)
-        k_res<DIM, true, false><<<g, kT, 0, st>>>(L, LC, sg, xp(l), C.x, cw, rp(l), M.res, nullptr,
-                                                  sk);
-      else
-        k_res<DIM, false, false><<<g, kT, 0, st>>>(L, LC, sg, xp(l), nullptr, 0.f, rp(l), M.res,
-                                                   nullptr, sk);
+      level_res<DIM>(M, LC, xp(l), ec, cw, rp(l), M.res, nullptr, sk, st);
       const bool last = (l == 0 && q == W.nu - 1);
-      if (last && hook)
-        k_sm<DIM, SM_ADD, true><<<g, kT, 0, st>>>(L, LC, sg, K, M.res, ec, cw, xp(l), -1, sk, rp(l),
-                                                  *hook);
-      else
-        k_sm<DIM, SM_ADD, false><<<g, kT, 0, st>>>(L, LC, sg, K, M.res, ec, cw, xp(l), -1,
-                                                   last ? sk : -1, rp(l), Hook{});
+      level_sm<DIM>(M, LC, K, false, M.res, ec, cw, xp(l), -1, last ? sk : -1, rp(l),
+                    last ? hook : nullptr, st);
       launches += 2;
     }
   }
@@ -831,29 +944,30 @@ double cycle_bytes(const MgHierarchy& H, const MgWeights& W) {
 // ------------------------------------------------------------ FCG kernels
 
 // r = b - A x, r32 = float(r); ||r|| decides whether the loop runs at all.
-template <int DIM>
-__global__ void __launch_bounds__(kT) k_fcg_init(OpView<double> A, Seg sg, FcgState* S,
-                                                 double* __restrict__ r, float* __restrict__ r32,
-                                                 double* partials, double* hist, int64_t hcap,
-                                                 Loop h) {
-  constexpr int PX = Tile<DIM>::PX, PY = Tile<DIM>::PY;
-  __shared__ double buf[2][PY + 2][PX + 2];
+template <int DIM, int CX>
+__global__ void __launch_bounds__(kT, 2) k_fcg_init(OpView<double> A, Seg sg, FcgState* S,
+                                                    double* __restrict__ r, float* __restrict__ r32,
+                                                    double* partials, double* hist, int64_t hcap,
+                                                    Loop h) {
+  constexpr int TX = Tile<DIM>::TX, TY = Tile<DIM>::TY;
+  __shared__ double buf[2][Rows<TY>::N][TX * CX + 2];
   const double* __restrict__ b = S->b;
   const double* __restrict__ x = S->x;
   double acc[1] = {0.0};
   auto val = [&](int i, int j, int k) { return x[i + (int64_t)A.nx * (j + (int64_t)A.ny * k)]; };
   for_runs(sg, A.nz, [&](int tix, int tiy, int k0, int k1) {
-    march7<double, PX, PY>(A.nx, A.ny, A.nz, tix, tiy, k0, k1, buf, val,
-                           [&](bool act, int i, int j, int k, double v, double w, double e,
-                               double s, double n, double bo, double t) {
-                             if (!act) return;
-                             const int64_t c = i + (int64_t)A.nx * (j + (int64_t)A.ny * k);
-                             const double rn =
-                                 b[c] - apply_coef(load_coef(A, i, j, k), v, w, e, s, n, bo, t);
-                             r[c] = rn;
-                             r32[c] = (float)rn;
-                             acc[0] += rn * rn;
-                           });
+    march7<double, TX, TY, CX>(
+        A.nx, A.ny, A.nz, tix, tiy, k0, k1, buf, val,
+        [&](int, bool act, int i, int j, int k, double v, double w, double e, double s, double n,
+            double bo, double t) {
+          if (!act) return;
+          const int64_t c = i + (int64_t)A.nx * (j + (int64_t)A.ny * k);
+          const double rn = b[c] - apply_coef(load_coef(A, i, j, k), v, w, e, s, n, bo, t);
+          r[c] = rn;
+          r32[c] = (float)rn;
+          acc[0] += rn * rn;
+        },
+        [](int) {});
   });
   reduce_last<1>(acc, partials, &S->ticket, [&](const double* tot) {
     const double b0 = sqrt(tot[0]);
@@ -879,13 +993,14 @@ __global__ void __launch_bounds__(kT) k_fcg_init(OpView<double> A, Seg sg, FcgSt
 
 // p = z - beta p_old (p = z on the first iteration), q = A p; p.q and p.r
 // give alpha.  p alternates between two buffers by iteration parity.
-template <int DIM>
-__global__ void __launch_bounds__(kT) k_fcg_dir(OpView<double> A, Seg sg, FcgState* S,
-                                                const float* __restrict__ z, double* P0, double* P1,
-                                                double* __restrict__ q, const double* __restrict__ r,
-                                                double* partials, Loop h) {
-  constexpr int PX = Tile<DIM>::PX, PY = Tile<DIM>::PY;
-  __shared__ double buf[2][PY + 2][PX + 2];
+template <int DIM, int CX>
+__global__ void __launch_bounds__(kT, 2) k_fcg_dir(OpView<double> A, Seg sg, FcgState* S,
+                                                   const float* __restrict__ z, double* P0,
+                                                   double* P1, double* __restrict__ q,
+                                                   const double* __restrict__ r, double* partials,
+                                                   Loop h) {
+  constexpr int TX = Tile<DIM>::TX, TY = Tile<DIM>::TY;
+  __shared__ double buf[2][Rows<TY>::N][TX * CX + 2];
   if (S->done) return;
   const long long it = S->it;
   const bool first = (it == 0);
@@ -898,17 +1013,19 @@ __global__ void __launch_bounds__(kT) k_fcg_dir(OpView<double> A, Seg sg, FcgSta
   };
   double acc[2] = {0.0, 0.0};
   for_runs(sg, A.nz, [&](int tix, int tiy, int k0, int k1) {
-    march7<double, PX, PY>(A.nx, A.ny, A.nz, tix, tiy, k0, k1, buf, val,
-                           [&](bool act, int i, int j, int k, double v, double w, double e,
-                               double s, double n, double bo, double t) {
-                             if (!act) return;
-                             const int64_t c = i + (int64_t)A.nx * (j + (int64_t)A.ny * k);
-                             const double aq = apply_coef(load_coef(A, i, j, k), v, w, e, s, n, bo, t);
-                             pn[c] = v;
-                             q[c] = aq;
-                             acc[0] += v * aq;
-                             acc[1] += v * r[c];
-                           });
+    march7<double, TX, TY, CX>(
+        A.nx, A.ny, A.nz, tix, tiy, k0, k1, buf, val,
+        [&](int, bool act, int i, int j, int k, double v, double w, double e, double s, double n,
+            double bo, double t) {
+          if (!act) return;
+          const int64_t c = i + (int64_t)A.nx * (j + (int64_t)A.ny * k);
+          const double aq = apply_coef(load_coef(A, i, j, k), v, w, e, s, n, bo, t);
+          pn[c] = v;
+          q[c] = aq;
+          acc[0] += v * aq;
+          acc[1] += v * r[c];
+        },
+        [](int) {});
   });
   reduce_last<2>(acc, partials, &S->ticket, [&](const double* tot) {
     const double pq = tot[0], pr = tot[1];
@@ -1102,20 +1219,37 @@ namespace {
 // Blocks of the widest reduction launch (one partial per block and value).
 int64_t partial_slots(const FineOperator&) { return kMaxBlocks; }
 
-template <int DIM>
-Seg fine_seg(const FineOperator& op) {
-  return make_seg<DIM>(op.A.nx, op.A.ny, op.A.nz);
+template <int DIM, int CX>
+void launch_init_t(LearnedSolver* s, const FineOperator& op, Loop h, cudaStream_t st) {
+  const Seg sg = make_seg<DIM, CX>(op.A.nx, op.A.ny, op.A.nz);
+  k_fcg_init<DIM, CX><<<seg_grid(sg), kT, 0, st>>>(op.A, sg, s->S, s->r, s->r32, s->partials,
+                                                   s->hist, s->hist_cap, h);
+}
+
+template <int DIM, int CX>
+void launch_dir_t(LearnedSolver* s, const FineOperator& op, Loop h, cudaStream_t st) {
+  const Seg sg = make_seg<DIM, CX>(op.A.nx, op.A.ny, op.A.nz);
+  k_fcg_dir<DIM, CX><<<seg_grid(sg), kT, 0, st>>>(op.A, sg, s->S, s->z32, s->p0, s->p1, s->q, s->r,
+                                                  s->partials, h);
 }
 
 void launch_init(LearnedSolver* s, const FineOperator& op, Loop h, cudaStream_t st) {
   if (op.dim == 2) {
-    const Seg sg = fine_seg<2>(op);
-    k_fcg_init<2><<<seg_grid(sg), kT, 0, st>>>(op.A, sg, s->S, s->r, s->r32, s->partials, s->hist,
-                                               s->hist_cap, h);
+    if (wide<2>(op.A.nx)) launch_init_t<2, 4>(s, op, h, st);
+    else launch_init_t<2, 1>(s, op, h, st);
   } else {
-    const Seg sg = fine_seg<3>(op);
-    k_fcg_init<3><<<seg_grid(sg), kT, 0, st>>>(op.A, sg, s->S, s->r, s->r32, s->partials, s->hist,
-                                               s->hist_cap, h);
+    if (wide<3>(op.A.nx)) launch_init_t<3, 4>(s, op, h, st);
+    else launch_init_t<3, 1>(s, op, h, st);
+  }
+}
+
+void launch_dir(LearnedSolver* s, const FineOperator& op, Loop h, cudaStream_t st) {
+  if (op.dim == 2) {
+    if (wide<2>(op.A.nx)) launch_dir_t<2, 4>(s, op, h, st);
+    else launch_dir_t<2, 1>(s, op, h, st);
+  } else {
+    if (wide<3>(op.A.nx)) launch_dir_t<3, 4>(s, op, h, st);
+    else launch_dir_t<3, 1>(s, op, h, st);
   }
 }
 
@@ -1124,18 +1258,9 @@ void launch_init(LearnedSolver* s, const FineOperator& op, Loop h, cudaStream_t 
 int enqueue_body(LearnedSolver* s, const FineOperator& op, Loop h, cudaStream_t st) {
   const int64_t skip = op.pinned ? op.ref : -1;
   const Hook hk{s->q, s->partials, s->S, h};
-  int nv;
-  if (op.dim == 2) {
-    nv = enqueue_cycle<2>(*s->H, s->W, s->r32, s->z32, skip, &hk, st);
-    const Seg sg = fine_seg<2>(op);
-    k_fcg_dir<2><<<seg_grid(sg), kT, 0, st>>>(op.A, sg, s->S, s->z32, s->p0, s->p1, s->q, s->r,
-                                              s->partials, h);
-  } else {
-    nv = enqueue_cycle<3>(*s->H, s->W, s->r32, s->z32, skip, &hk, st);
-    const Seg sg = fine_seg<3>(op);
-    k_fcg_dir<3><<<seg_grid(sg), kT, 0, st>>>(op.A, sg, s->S, s->z32, s->p0, s->p1, s->q, s->r,
-                                              s->partials, h);
-  }
+  const int nv = op.dim == 2 ? enqueue_cycle<2>(*s->H, s->W, s->r32, s->z32, skip, &hk, st)
+                             : enqueue_cycle<3>(*s->H, s->W, s->r32, s->z32, skip, &hk, st);
+  launch_dir(s, op, h, st);
   k_fcg_update<<<flat_grid(s->cells), 256, 0, st>>>(s->cells, s->S, s->r, s->r32, s->p0, s->p1,
                                                     s->q, s->partials, s->hist, s->hist_cap, h);
   return nv + 2;
@@ -1208,11 +1333,12 @@ cfdb_status capture_graph(cfdb_context* ctx, LearnedSolver* s, const FineOperato
 
 }  // namespace
 
-cfdb_status learned_solve(cfdb_context* ctx, LearnedSolver* s, const FineOperator& op,
-                          uint64_t version, const MgWeights& W, const double* b, double* x,
-                          double abs_tol, double rel_tol, int64_t max_it, int64_t hist_cap,
-                          LearnedOutcome* out) {
-  std::memset(out, 0, sizeof(*out));
+namespace {
+
+// Builds (new shape) or refreshes (new coefficient version) the hierarchy and
+// the FCG vectors; *recapture tells whether the solve graph must be rebuilt.
+cfdb_status ensure_state(cfdb_context* ctx, LearnedSolver* s, const FineOperator& op,
+                         uint64_t version, bool* recapture_out) {
   const int64_t cells = (int64_t)op.n[0] * op.n[1] * op.n[2];
   const bool same_shape = s->H && s->dim == op.dim && s->n[0] == op.n[0] && s->n[1] == op.n[1] &&
                           s->n[2] == op.n[2];
@@ -1255,6 +1381,33 @@ cfdb_status learned_solve(cfdb_context* ctx, LearnedSolver* s, const FineOperato
     if (st != CFDB_OK) return st;
     s->version = version;
   }
+  *recapture_out = recapture;
+  return CFDB_OK;
+}
+
+}  // namespace
+
+cfdb_status learned_hierarchy(cfdb_context* ctx, LearnedSolver* s, const FineOperator& op,
+                              uint64_t version, const MgHierarchy** out) {
+  bool recapture = false;
+  cfdb_status st = ensure_state(ctx, s, op, version, &recapture);
+  if (st != CFDB_OK) return st;
+  if (recapture) s->free_graph();
+  *out = s->H;
+  return CFDB_OK;
+}
+
+cfdb_status learned_solve(cfdb_context* ctx, LearnedSolver* s, const FineOperator& op,
+                          uint64_t version, const MgWeights& W, const double* b, double* x,
+                          double abs_tol, double rel_tol, int64_t max_it, int64_t hist_cap,
+                          LearnedOutcome* out) {
+  std::memset(out, 0, sizeof(*out));
+  bool recapture = false;
+  {
+    cfdb_status st = ensure_state(ctx, s, op, version, &recapture);
+    if (st != CFDB_OK) return st;
+  }
+  if (!s->exec) recapture = true;
   const int64_t want_hist = std::max<int64_t>(hist_cap, 1);
   if (s->hist_cap < want_hist) {
     cudaFree(s->hist);
@@ -1377,6 +1530,37 @@ cfdb_status cfdb_mg_get_weights(cfdb_context* ctx, int dim, int* levels, int* nu
   if (kernels) std::memcpy(kernels, W.w, sizeof(W.w));
   if (coarse_weights) std::memcpy(coarse_weights, W.c, sizeof(W.c));
   return CFDB_OK;
+}
+
+cfdb_status cfdb_mg_apply(cfdb_context* ctx, cfdb_poperator* op, const float* r_host,
+                          float* z_host) {
+  if (!ctx || !op || !r_host || !z_host) return CFDB_ERR_INVALID_ARGUMENT;
+  CFDB_CUDA(ctx, cudaSetDevice(ctx->device));
+  FineOperator fo;
+  LearnedSolver* solver = nullptr;
+  uint64_t version = 0;
+  poperator_learned(op, &fo, &solver, &version);
+  const MgHierarchy* H = nullptr;
+  cfdb_status st = learned_hierarchy(ctx, solver, fo, version, &H);
+  if (st != CFDB_OK) return st;
+  const int64_t n = H->L[0].cells;
+  float *r = nullptr, *z = nullptr;
+  CFDB_CUDA(ctx, cudaMalloc((void**)&r, sizeof(float) * n));
+  if (cudaMalloc((void**)&z, sizeof(float) * n) != cudaSuccess) {
+    cudaFree(r);
+    return set_error(ctx, CFDB_ERR_OUT_OF_MEMORY, "mg_apply buffers");
+  }
+  cudaStream_t s = ctx->stream;
+  cudaError_t e = cudaMemcpyAsync(r, r_host, sizeof(float) * n, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) {
+    st = mg_apply(ctx, *H, mg_context_weights(ctx, fo.dim), r, z, fo.pinned ? fo.ref : -1);
+    if (st == CFDB_OK) e = cudaMemcpyAsync(z_host, z, sizeof(float) * n, cudaMemcpyDeviceToHost, s);
+    if (st == CFDB_OK && e == cudaSuccess) e = cudaStreamSynchronize(s);
+  }
+  cudaFree(r);
+  cudaFree(z);
+  if (e != cudaSuccess) return cuda_error(ctx, e, "mg_apply", __FILE__, __LINE__);
+  return st;
 }
 
 cfdb_status cfdb_mg_reset_weights(cfdb_context* ctx, int dim, int trained) {

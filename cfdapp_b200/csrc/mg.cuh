@@ -117,8 +117,15 @@ cfdb_status learned_solve(cfdb_context* ctx, LearnedSolver* s, const FineOperato
                           uint64_t version, const MgWeights& W, const double* b, double* x,
                           double abs_tol, double rel_tol, int64_t max_it, int64_t hist_cap,
                           LearnedOutcome* out);
+// The solver's hierarchy for `op`, built or refreshed as a solve would.
+cfdb_status learned_hierarchy(cfdb_context* ctx, LearnedSolver* s, const FineOperator& op,
+                              uint64_t version, const MgHierarchy** out);
 // Copies the first m residual-history entries of the last solve to the host.
 cfdb_status learned_history(cfdb_context* ctx, LearnedSolver* s, double* host, int64_t m);
+
+// Kernel-space taps of level l (2D weight sets keep their 3x3 taps in the
+// middle plane of the 27; kernel space maps real y to z).
+void mg_kernel_taps(const MgWeights& W, int l, float out[kMgTaps]);
 
 // The weights shipped with the library (trained), or the defaults when none.
 MgWeights mg_builtin_weights(int dim);

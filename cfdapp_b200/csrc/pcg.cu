@@ -29,6 +29,7 @@
 #include "cfdb_internal.cuh"
 #include "grid_sync.cuh"
 #include "mg.cuh"
+#include "pcg_internal.cuh"
 #include "poperator.cuh"
 #include "tile.cuh"
 #include "tma.cuh"
@@ -742,23 +743,12 @@ cfdb_status solve_learned(cfdb_context* ctx, cfdb_poperator* op, const cfdb_line
                           cfdb_linear_result* res) {
   const cfdb_grid& g = op->grid;
   FineOperator fo;
-  std::memset(&fo, 0, sizeof(fo));
-  fo.dim = g.dim;
-  fo.n[0] = op->knx;
-  fo.n[1] = op->kny;
-  fo.n[2] = op->knz;
-  fo.A = view<double>(op);
-  for (int q = 0; q < 3; ++q) {
-    const bool active = g.dim == 3 || q != 1;  // 2D kernel space has no y-faces
-    fo.full[q] = active ? op->f64[q] : nullptr;
-    fo.table[q] = active ? op->t64[q] : nullptr;
-  }
-  fo.pinned = op->pinned;
-  fo.ref = op->ref;
-  if (!op->learned) op->learned = learned_create();
+  LearnedSolver* solver = nullptr;
+  uint64_t version = 0;
+  poperator_learned(op, &fo, &solver, &version);
   const int64_t cap = std::min<int64_t>(s->max_iterations, 100000);
   LearnedOutcome o;
-  cfdb_status st = learned_solve(ctx, op->learned, fo, op->version, mg_context_weights(ctx, g.dim),
+  cfdb_status st = learned_solve(ctx, solver, fo, version, mg_context_weights(ctx, g.dim),
                                  b, x, s->abs_tol, s->rel_tol, cap,
                                  std::max<int64_t>(history_cap, 1), &o);
   if (st != CFDB_OK) return st;
@@ -770,7 +760,7 @@ cfdb_status solve_learned(cfdb_context* ctx, cfdb_poperator* op, const cfdb_line
   res->krylov_bytes += o.bytes;
   res->krylov_launches += 1;
   if (history && history_cap > 0) {
-    st = learned_history(ctx, op->learned, history, std::min<int64_t>(history_cap, o.iterations + 1));
+    st = learned_history(ctx, solver, history, std::min<int64_t>(history_cap, o.iterations + 1));
     if (st != CFDB_OK) return st;
   }
   const bool stalled = o.status == kLearnedStagnated ||
@@ -931,6 +921,26 @@ cfdb_status poperator_bind_faces(cfdb_context* ctx, cfdb_poperator* op, const do
   CFDB_CHECK_LAUNCH(ctx);
   count_launch(ctx, fp32 ? 2 + g.dim : 1);
   return CFDB_OK;
+}
+
+void poperator_learned(cfdb_poperator* op, FineOperator* fo, LearnedSolver** solver,
+                       uint64_t* version) {
+  std::memset(fo, 0, sizeof(*fo));
+  fo->dim = op->grid.dim;
+  fo->n[0] = op->knx;
+  fo->n[1] = op->kny;
+  fo->n[2] = op->knz;
+  fo->A = view<double>(op);
+  for (int q = 0; q < 3; ++q) {
+    const bool active = op->grid.dim == 3 || q != 1;  // 2D kernel space has no y-faces
+    fo->full[q] = active ? op->f64[q] : nullptr;
+    fo->table[q] = active ? op->t64[q] : nullptr;
+  }
+  fo->pinned = op->pinned;
+  fo->ref = op->ref;
+  if (!op->learned) op->learned = learned_create();
+  *solver = op->learned;
+  *version = op->version;
 }
 
 }  // namespace cfdb

@@ -295,6 +295,24 @@ CFDB_API cfdb_status cfdb_mg_get_weights(cfdb_context* ctx, int dim, int* levels
                                          float* coarse_weights);
 /* trained = 1: the weights shipped with the library; 0: untrained damped Jacobi. */
 CFDB_API cfdb_status cfdb_mg_reset_weights(cfdb_context* ctx, int dim, int trained);
+/* No counterpart in the reference.  z = M r: one application of the learned
+ * V-cycle of `op` (the context's weights) through the solve's own kernels;
+ * host FP32 vectors in op's cell order (r[reference cell] reads as 0 and
+ * z[reference cell] = r[reference cell] when the operator is pinned). */
+CFDB_API cfdb_status cfdb_mg_apply(cfdb_context* ctx, cfdb_poperator* op, const float* r_host,
+                                   float* z_host);
+/* No counterpart in the reference.  Training signal of the learned V-cycle on
+ * the GPU: for `nsamples` error fields e (host, nsamples x cells FP32, cell
+ * order of `op`; e[reference cell] is taken as 0 when the operator is pinned)
+ * the loss  mean ||e - M A e||_A^2 / ||e||_A^2  of the context's current
+ * weights for op's dimension, and its exact gradient by reverse-mode
+ * differentiation: grad_kernels[16*27] (tied taps t and 26-t receive the same
+ * summed value; 2D sets use taps 9..17) and grad_coarse[16], per level that
+ * owns weights (levels deeper than the weight set's count add into the last).
+ * Either gradient pointer may be NULL. */
+CFDB_API cfdb_status cfdb_mg_loss_grad(cfdb_context* ctx, cfdb_poperator* op, int nsamples,
+                                       const float* e_host, double* loss, double* grad_kernels,
+                                       double* grad_coarse);
 
 /* ------------------------------------------------------ allocation-free solve */
 

@@ -155,3 +155,80 @@ def test_weights_api(ctx):
     ctx.mg_reset_weights(3, trained=False)
     assert ctx.mg_get_weights(3)["kernels"][0, 13] == np.float32(0.8)
     ctx.mg_reset_weights(3, trained=True)
+
+
+# ------------------------------------------------ the network against its oracle
+from oracle import mg_oracle as MO  # noqa: E402
+
+
+def _face_op(ctx, dim, n, seed):
+    from cfdapp_b200.cfdb import POperator
+    fc = MO.random_faces(dim, n, seed)
+    op = POperator(ctx, dim, n, face_coeff=fc, pinned=True, reference_cell=0)
+    dims, f = MO.kernel_faces(dim, n, fc)
+    return op, MO.hierarchy(dims, f, dim)
+
+
+@pytest.mark.parametrize("dim,n", [(2, (40, 36)), (3, (24, 20, 18))])
+def test_vcycle_kernels_match_oracle(ctx, dim, n):
+    """One application of the solve's tiled V-cycle (grid levels + the
+    block-resident coarse levels) against the FP64 restatement."""
+    op, H = _face_op(ctx, dim, n, 21)
+    k, c = MO.random_weights(dim, 2, 22)
+    k32, c32 = k.astype(np.float32), c.astype(np.float32)
+    ctx.mg_set_weights(dim, k32, c32, nu=2, coarse_sweeps=10)
+    try:
+        r = np.random.default_rng(23).normal(size=int(np.prod(n))).astype(np.float32)
+        z = op.mg_apply(r)
+        V = MO.VCycle(dim, H, k32.astype(np.float64), c32.astype(np.float64), nu=2,
+                      coarse_sweeps=10)
+        zr = V.apply(r.astype(np.float64), pin=0)
+        assert _rel(z.astype(np.float64), zr) <= 2e-5
+    finally:
+        ctx.mg_reset_weights(dim, trained=True)
+
+
+@pytest.mark.parametrize("dim,n", [(2, (20, 18)), (3, (10, 8, 8))])
+def test_gradient_matches_finite_differences(ctx, dim, n):
+    """The GPU reverse-mode gradient of the training loss against central
+    differences of the FP64 oracle loss (h = 1e-4 on every free weight)."""
+    op, H = _face_op(ctx, dim, n, 31)
+    k, c = MO.random_weights(dim, 2, 32)
+    k = k.astype(np.float32).astype(np.float64)
+    c = c.astype(np.float32).astype(np.float64)
+    nu, sweeps = 2, 6
+    ctx.mg_set_weights(dim, k.astype(np.float32), c.astype(np.float32), nu=nu,
+                       coarse_sweeps=sweeps)
+    e = np.random.default_rng(33).normal(size=(3, int(np.prod(n)))).astype(np.float32)
+    try:
+        loss, gk, gc = op.mg_loss_grad(e)
+    finally:
+        ctx.mg_reset_weights(dim, trained=True)
+
+    def oracle_loss(kk, cc):
+        V = MO.VCycle(dim, H, kk, cc, nu=nu, coarse_sweeps=sweeps)
+        return float(np.mean([V.loss(ei.astype(np.float64), pin=0) for ei in e]))
+
+    assert loss == pytest.approx(oracle_loss(k, c), rel=1e-4)
+    h = 1e-4
+    g_gpu, g_fd = [], []
+    for l in range(2):
+        for t in MO.free_params(dim):
+            kp, km = k.copy(), k.copy()
+            for kk, sgn in ((kp, 1.0), (km, -1.0)):
+                kk[l, t] += sgn * h
+                if t != 13:
+                    kk[l, 26 - t] += sgn * h
+            g_fd.append((oracle_loss(kp, c) - oracle_loss(km, c)) / (2 * h))
+            g_gpu.append(gk[l, t])
+        cp, cm = c.copy(), c.copy()
+        cp[l] += h
+        cm[l] -= h
+        g_fd.append((oracle_loss(k, cp) - oracle_loss(k, cm)) / (2 * h))
+        g_gpu.append(gc[l])
+    g_gpu, g_fd = np.array(g_gpu), np.array(g_fd)
+    assert np.linalg.norm(g_gpu - g_fd) <= 2e-3 * np.linalg.norm(g_fd)
+    # tied taps carry the same gradient
+    for l in range(2):
+        for t in MO.free_params(dim):
+            assert gk[l, t] == gk[l, 26 - t]
