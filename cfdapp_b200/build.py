@@ -42,7 +42,7 @@ def _sources():
 
 
 def _deps():
-    return (_sources() + glob.glob(os.path.join(CSRC, "*.cuh")) +
+    return (_sources() + glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.inc")) +
             [os.path.join(ROOT, "include", "cfdb.h")])
 
 

@@ -232,3 +232,27 @@ def test_gradient_matches_finite_differences(ctx, dim, n):
     for l in range(2):
         for t in MO.free_params(dim):
             assert gk[l, t] == gk[l, 26 - t]
+
+
+# ---------------------------------------------------- what training buys
+@pytest.mark.parametrize("dim,n,gain", [(2, 512, 0.8), (3, 96, 0.6)])
+def test_trained_weights_cut_iterations(ctx, dim, n, gain):
+    """The shipped (GPU-trained) weights need clearly fewer FCG iterations
+    than the untrained network (damped Jacobi layers) on systems larger than
+    any seen in training (128^2 / 32^3): the isolated p' system and a
+    smooth-response one."""
+    from cfdapp_b200.cfdb import POperator
+    from cfdapp_b200.mgtrain import random_operator_faces
+    b = O.synth_rhs(dim, n)
+    ops = [POperator(ctx, dim, [n] * dim),
+           POperator(ctx, dim, [n] * dim,
+                     face_coeff=random_operator_faces(dim, [n] * dim, np.random.default_rng(5)))]
+    for op in ops:
+        ctx.mg_reset_weights(dim, trained=False)
+        untrained = op.solve(b, _settings())
+        ctx.mg_reset_weights(dim, trained=True)
+        trained = op.solve(b, _settings())
+        assert untrained.status == trained.status == "Converged"
+        assert trained.fallback_iterations == 0
+        assert trained.iterations <= gain * untrained.iterations, (trained.iterations,
+                                                                   untrained.iterations)
