@@ -216,13 +216,6 @@ int seg_grid(const Seg& s) {
 }
 
 // Four cells per thread where the level is wide enough.
-// (2D rows stay at one cell per thread: with only nx/1024 tiles per row the
-// plane runs get too short to hide the z-halo reloads.)
-template <int DIM>
-bool wide(int nx) {
-  return DIM == 3 && nx >= Tile<DIM>::TX * 4;
-}
-
 // f(tix, tiy, k0, k1) for every plane run of this block.
 template <class F>
 __device__ __forceinline__ void for_runs(const Seg& sg, int nz, F f) {
@@ -832,6 +825,8 @@ CoarsePlan coarse_plan(const MgHierarchy& H, const MgWeights& W) {
   return P;
 }
 
+#include "mg_quad.cuh"
+
 // Launchers of one level's passes, with the cells-per-thread choice.
 template <int DIM, int CX>
 struct LevelOps {
@@ -864,16 +859,37 @@ struct LevelOps {
 template <int DIM>
 void level_res(const MgLevel& M, const LV& LC, const float* x, const float* ec, float cw,
                const float* r, float* res, float* rc, int64_t skip, cudaStream_t st) {
-  if (wide<DIM>(M.n[0])) LevelOps<DIM, 4>::res(M, LC, x, ec, cw, r, res, rc, skip, st);
-  else LevelOps<DIM, 1>::res(M, LC, x, ec, cw, r, res, rc, skip, st);
+  if (quad_ok<DIM>(M.n[0])) {
+    const Seg sg = make_quad_seg<DIM>(M.n[0], M.n[1], M.n[2]);
+    const int g = quad_grid<DIM>(sg);
+    constexpr int T = Quad<DIM>::TX * Quad<DIM>::TY;
+    const LV L = lv(M);
+    if (rc) k_res_q<DIM, false, true><<<g, T, 0, st>>>(L, LC, sg, x, ec, cw, r, res, rc, skip);
+    else if (ec) k_res_q<DIM, true, false><<<g, T, 0, st>>>(L, LC, sg, x, ec, cw, r, res, rc, skip);
+    else k_res_q<DIM, false, false><<<g, T, 0, st>>>(L, LC, sg, x, ec, cw, r, res, rc, skip);
+  } else {
+    LevelOps<DIM, 1>::res(M, LC, x, ec, cw, r, res, rc, skip, st);
+  }
 }
 
 template <int DIM>
 void level_sm(const MgLevel& M, const LV& LC, const Kern& K, bool first, const float* src,
               const float* ec, float cw, float* x, int64_t skip, int64_t pin, const float* r,
               const Hook* hook, cudaStream_t st) {
-  if (wide<DIM>(M.n[0])) LevelOps<DIM, 4>::sm(M, LC, K, first, src, ec, cw, x, skip, pin, r, hook, st);
-  else LevelOps<DIM, 1>::sm(M, LC, K, first, src, ec, cw, x, skip, pin, r, hook, st);
+  if (quad_ok<DIM>(M.n[0])) {
+    const Seg sg = make_quad_seg<DIM>(M.n[0], M.n[1], M.n[2]);
+    const int g = quad_grid<DIM>(sg);
+    constexpr int T = Quad<DIM>::TX * Quad<DIM>::TY;
+    const LV L = lv(M);
+    if (first)
+      k_sm_q<DIM, SM_FIRST, false><<<g, T, 0, st>>>(L, LC, sg, K, src, ec, cw, x, skip, pin, r, Hook{});
+    else if (hook)
+      k_sm_q<DIM, SM_ADD, true><<<g, T, 0, st>>>(L, LC, sg, K, src, ec, cw, x, skip, pin, r, *hook);
+    else
+      k_sm_q<DIM, SM_ADD, false><<<g, T, 0, st>>>(L, LC, sg, K, src, ec, cw, x, skip, pin, r, Hook{});
+  } else {
+    LevelOps<DIM, 1>::sm(M, LC, K, first, src, ec, cw, x, skip, pin, r, hook, st);
+  }
 }
 
 // Enqueues z = M r (level-0 FP32 vectors) on `st`; returns the number of
@@ -1216,8 +1232,9 @@ void learned_destroy(LearnedSolver* s) {
 
 namespace {
 
-// Blocks of the widest reduction launch (one partial per block and value).
-int64_t partial_slots(const FineOperator&) { return kMaxBlocks; }
+// Blocks of the widest reduction launch (one partial per block and value):
+// 2D quad passes run up to 32 blocks of 64 threads per SM.
+int64_t partial_slots(const FineOperator&) { return std::max(kMaxBlocks, 148 * 32); }
 
 template <int DIM, int CX>
 void launch_init_t(LearnedSolver* s, const FineOperator& op, Loop h, cudaStream_t st) {
@@ -1234,21 +1251,23 @@ void launch_dir_t(LearnedSolver* s, const FineOperator& op, Loop h, cudaStream_t
 }
 
 void launch_init(LearnedSolver* s, const FineOperator& op, Loop h, cudaStream_t st) {
-  if (op.dim == 2) {
-    if (wide<2>(op.A.nx)) launch_init_t<2, 4>(s, op, h, st);
-    else launch_init_t<2, 1>(s, op, h, st);
-  } else {
-    if (wide<3>(op.A.nx)) launch_init_t<3, 4>(s, op, h, st);
-    else launch_init_t<3, 1>(s, op, h, st);
-  }
+  if (op.dim == 2) launch_init_t<2, 1>(s, op, h, st);
+  else launch_init_t<3, 1>(s, op, h, st);
+}
+
+template <int DIM>
+void launch_dir_q(LearnedSolver* s, const FineOperator& op, Loop h, cudaStream_t st) {
+  const Seg sg = make_quad_seg<DIM>(op.A.nx, op.A.ny, op.A.nz);
+  k_fcg_dir_q<DIM><<<quad_grid<DIM>(sg), Quad<DIM>::TX * Quad<DIM>::TY, 0, st>>>(
+      op.A, sg, s->S, s->z32, s->p0, s->p1, s->q, s->r, s->partials, h);
 }
 
 void launch_dir(LearnedSolver* s, const FineOperator& op, Loop h, cudaStream_t st) {
   if (op.dim == 2) {
-    if (wide<2>(op.A.nx)) launch_dir_t<2, 4>(s, op, h, st);
+    if (quad_ok<2>(op.A.nx)) launch_dir_q<2>(s, op, h, st);
     else launch_dir_t<2, 1>(s, op, h, st);
   } else {
-    if (wide<3>(op.A.nx)) launch_dir_t<3, 4>(s, op, h, st);
+    if (quad_ok<3>(op.A.nx)) launch_dir_q<3>(s, op, h, st);
     else launch_dir_t<3, 1>(s, op, h, st);
   }
 }
