@@ -565,28 +565,39 @@ __device__ __forceinline__ float lap_s(const LV& M, int i, int j, int k, int c, 
   return apply7(co, x[c], w, e, s, n, b, t);
 }
 
-// sum_o K[o] isq(c+o) v(c+o)
-template <int DIM>
+// sum_o K[o] u(c+o), or with SCALE sum_o K[o] isq(c+o) u(c+o)
+template <int DIM, bool SCALE>
 __device__ __forceinline__ float conv_s(const LV& M, const Kern& K, int i, int j, int k,
-                                        const float* v) {
+                                        const float* u) {
   float s = 0.f;
+#pragma unroll
   for (int dk = -1; dk <= 1; ++dk) {
     const int kk = k + dk;
     if (kk < 0 || kk >= M.nz) continue;
+#pragma unroll
     for (int dj = (DIM == 2 ? 0 : -1); dj <= (DIM == 2 ? 0 : 1); ++dj) {
       const int jj = j + dj;
       if (jj < 0 || jj >= M.ny) continue;
+      const int rowq = M.nx * (jj + M.ny * kk);
+#pragma unroll
       for (int di = -1; di <= 1; ++di) {
         const int ii = i + di;
         if (ii < 0 || ii >= M.nx) continue;
-        const int q = ii + M.nx * (jj + M.ny * kk);
-        s += K.w[(dk + 1) * 9 + (dj + 1) * 3 + (di + 1)] * (M.isq[q] * v[q]);
+        const int q = ii + rowq;
+        const float v = SCALE ? M.isq[q] * u[q] : u[q];
+        s += K.w[(dk + 1) * 9 + (dj + 1) * 3 + (di + 1)] * v;
       }
     }
   }
   return s;
 }
 
+// The block-resident tail of the V-cycle: levels cf.. with their faces,
+// scales and vectors in shared memory.  Same layers as the grid kernels;
+// the smoothing residual is stored pre-scaled (u = D^-1/2 res), cell
+// coordinates come from a float reciprocal (exact below 2^22 cells), and the
+// coarsest level's damped-Jacobi sweeps run on only the warps that own its
+// cells (a named barrier instead of the whole block).
 template <int DIM>
 __global__ void __launch_bounds__(kCoarseThreads) k_coarse(CoarsePlan P) {
   extern __shared__ float4 smem4[];
@@ -598,8 +609,12 @@ __global__ void __launch_bounds__(kCoarseThreads) k_coarse(CoarsePlan P) {
                        c.n[0] * c.n[1] * (c.n[2] + 1)};
     for (int a = 0; a < 3; ++a) {
       if (DIM == 2 && a == 1) continue;
-      for (int q = tid; q < nf[a]; q += nt) sm[c.off[a] + q] = c.f[a][q];
+      const float* src = c.f[a];
+      float* dst = sm + c.off[a];
+#pragma unroll 4
+      for (int q = tid; q < nf[a]; q += nt) dst[q] = src[q];
     }
+#pragma unroll 4
     for (int q = tid; q < c.cells; q += nt) sm[c.off[3] + q] = c.isq[q];
   }
   for (int q = tid; q < P.lv[0].cells; q += nt) sm[P.lv[0].off[5] + q] = P.lv[0].r_glob[q];
@@ -611,9 +626,12 @@ __global__ void __launch_bounds__(kCoarseThreads) k_coarse(CoarsePlan P) {
   };
   auto cells_of = [&](const LV& M, auto f) {
     const int cells = M.nx * M.ny * M.nz;
+    const float inx = 1.0f / (float)M.nx, iny = 1.0f / (float)M.ny;
     for (int c = tid; c < cells; c += nt) {
-      const int i = c % M.nx, rest = c / M.nx;
-      f(i, rest % M.ny, rest / M.ny, c);
+      const int rest = __float2int_rz(((float)c + 0.5f) * inx);
+      const int i = c - rest * M.nx;
+      const int k = __float2int_rz(((float)rest + 0.5f) * iny);
+      f(i, rest - k * M.ny, k, c);
     }
   };
   const int last = P.count - 1;
@@ -623,12 +641,12 @@ __global__ void __launch_bounds__(kCoarseThreads) k_coarse(CoarsePlan P) {
     const float* r = sm + P.lv[l].off[5];
     float* res = sm + P.lv[l].off[6];
     const Kern& K = P.K[l];
-    cells_of(M, [&](int i, int j, int k, int c) { x[c] = M.isq[c] * conv_s<DIM>(M, K, i, j, k, r); });
+    cells_of(M, [&](int i, int j, int k, int c) { x[c] = M.isq[c] * conv_s<DIM, true>(M, K, i, j, k, r); });
     __syncthreads();
     for (int s = 1; s < P.nu; ++s) {
-      cells_of(M, [&](int i, int j, int k, int c) { res[c] = r[c] - lap_s<DIM>(M, i, j, k, c, x); });
+      cells_of(M, [&](int i, int j, int k, int c) { res[c] = M.isq[c] * (r[c] - lap_s<DIM>(M, i, j, k, c, x)); });
       __syncthreads();
-      cells_of(M, [&](int i, int j, int k, int c) { x[c] += M.isq[c] * conv_s<DIM>(M, K, i, j, k, res); });
+      cells_of(M, [&](int i, int j, int k, int c) { x[c] += M.isq[c] * conv_s<DIM, false>(M, K, i, j, k, res); });
       __syncthreads();
     }
     cells_of(M, [&](int i, int j, int k, int c) { res[c] = r[c] - lap_s<DIM>(M, i, j, k, c, x); });
@@ -652,17 +670,32 @@ __global__ void __launch_bounds__(kCoarseThreads) k_coarse(CoarsePlan P) {
     float* x = sm + P.lv[last].off[4];
     const float* r = sm + P.lv[last].off[5];
     float* res = sm + P.lv[last].off[6];
-    cells_of(M, [&](int, int, int, int c) { x[c] = 0.f; });
-    __syncthreads();
-    for (int s = 0; s < P.sweeps; ++s) {
-      cells_of(M, [&](int i, int j, int k, int c) { res[c] = r[c] - lap_s<DIM>(M, i, j, k, c, x); });
-      __syncthreads();
-      cells_of(M, [&](int, int, int, int c) {
-        const float is = M.isq[c];
-        x[c] += 0.8f * (is * is) * res[c];
-      });
-      __syncthreads();
+    const int cells = M.nx * M.ny * M.nz;
+    const int nw = min(32, (cells + 31) / 32);  // warps that own the coarsest cells
+    if (tid < 32 * nw) {
+      auto wsync = [&]() {
+        if (nw == 1) __syncwarp();
+        else asm volatile("bar.sync 1, %0;" ::"r"(32 * nw) : "memory");
+      };
+      const float inx = 1.0f / (float)M.nx, iny = 1.0f / (float)M.ny;
+      for (int c = tid; c < cells; c += 32 * nw) x[c] = 0.f;
+      wsync();
+      for (int s = 0; s < P.sweeps; ++s) {
+        for (int c = tid; c < cells; c += 32 * nw) {
+          const int rest = __float2int_rz(((float)c + 0.5f) * inx);
+          const int i = c - rest * M.nx;
+          const int k = __float2int_rz(((float)rest + 0.5f) * iny);
+          res[c] = r[c] - lap_s<DIM>(M, i, rest - k * M.ny, k, c, x);
+        }
+        wsync();
+        for (int c = tid; c < cells; c += 32 * nw) {
+          const float is = M.isq[c];
+          x[c] += 0.8f * (is * is) * res[c];
+        }
+        wsync();
+      }
     }
+    __syncthreads();
   }
   for (int l = last - 1; l >= 0; --l) {
     const LV M = level(l);
@@ -676,9 +709,9 @@ __global__ void __launch_bounds__(kCoarseThreads) k_coarse(CoarsePlan P) {
     cells_of(M, [&](int i, int j, int k, int c) { x[c] += cw * ec[parent(Cc, i, j, k)]; });
     __syncthreads();
     for (int s = 0; s < P.nu; ++s) {
-      cells_of(M, [&](int i, int j, int k, int c) { res[c] = r[c] - lap_s<DIM>(M, i, j, k, c, x); });
+      cells_of(M, [&](int i, int j, int k, int c) { res[c] = M.isq[c] * (r[c] - lap_s<DIM>(M, i, j, k, c, x)); });
       __syncthreads();
-      cells_of(M, [&](int i, int j, int k, int c) { x[c] += M.isq[c] * conv_s<DIM>(M, K, i, j, k, res); });
+      cells_of(M, [&](int i, int j, int k, int c) { x[c] += M.isq[c] * conv_s<DIM, false>(M, K, i, j, k, res); });
       __syncthreads();
     }
   }

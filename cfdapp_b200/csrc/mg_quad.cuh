@@ -350,7 +350,7 @@ __global__ void __launch_bounds__(Quad<DIM>::TX* Quad<DIM>::TY)
 
 // The quad counterpart of the FCG direction pass (see k_fcg_dir).
 template <int DIM>
-__global__ void __launch_bounds__(Quad<DIM>::TX* Quad<DIM>::TY, 2)
+__global__ void __launch_bounds__(Quad<DIM>::TX* Quad<DIM>::TY, DIM == 3 ? 2 : 12)
     k_fcg_dir_q(OpView<double> A, Seg sg, FcgState* S, const float* __restrict__ z, double* P0,
                 double* P1, double* __restrict__ q, const double* __restrict__ r, double* partials,
                 Loop h) {
