@@ -147,3 +147,27 @@ def test_simple_failure_statuses(ctx):
     nan = np.zeros(case.cells())
     nan[3] = np.nan
     assert simple_solve(ctx, case, SIMPLESettings(max_iterations=5), u0=nan).status == "NonFiniteState"
+
+
+@pytest.mark.parametrize("name", ["cavity2d_16_jacobicg", "channel2d_32x8_central_rc",
+                                  "cavity2d_16_lud", "cavity3d_8_quick_rc"])
+def test_simple_with_learned_pressure_solver_matches_reference(ctx, name):
+    """The same SIMPLE runs with every p' system solved by the learned-
+    preconditioned FCG (to the same tolerance) land on the reference's fields."""
+    from cfdapp_b200.cfdb import simple_solve
+    g, meta = _golden(name)
+    args = meta["args"].replace("psolver=bicgstab", "psolver=cg")
+    args = " ".join(a for a in args.split() if not a.startswith("ppre="))
+    case, s = gpu_case_from_args(args + " psolver=cg ppre=learned_mg")
+    r = simple_solve(ctx, case, s)
+    assert r.status == meta["status"]
+    if meta["status"] == "Converged":
+        assert abs(r.iterations - meta["iterations"]) <= max(3, 0.03 * meta["iterations"])
+    else:
+        assert r.iterations == meta["iterations"]
+    # a run stopped early carries the p' solve tolerance into its fields
+    bar = 1e-6 if float(_kv(args).get("prel", 1e-8)) <= 1e-8 else 1e-3
+    for f in ("u", "v", "w", "p"):
+        if f in g.files:
+            assert _rel(getattr(r, f), g[f]) <= bar, f
+    assert _rel(r.flux, g["flux"]) <= bar
