@@ -551,6 +551,7 @@ def _simple_sigs(L):
     L.cfdb_simple_pressure_gradient.argtypes = [vp, dp, dp, dp]
     L.cfdb_simple_assemble_momentum.argtypes = [vp, C.c_int, dp, C.POINTER(dp), dp]
     L.cfdb_simple_iterate.argtypes = [vp, C.c_int64, dp, C.POINTER(_SimpleResult)]
+    L.cfdb_simple_pprime_faces.argtypes = [vp, dp, C.POINTER(C.c_int), C.POINTER(C.c_int64)]
 
 
 def _result(r: _SimpleResult, case, u, v, w, p, flux, hist) -> SIMPLEResult:
@@ -625,6 +626,15 @@ class Simple:
                                                                   _dp(rhs)),
                        "cfdb_simple_assemble_momentum")
         return diag, off, rhs
+
+    def pprime_faces(self):
+        """(D_f in global face order, pinned, reference cell) of the last p' system."""
+        f = np.zeros(self.case.faces())
+        pin, ref = C.c_int(), C.c_int64()
+        self.ctx.check(self.ctx.lib.cfdb_simple_pprime_faces(self._h, _dp(f), C.byref(pin),
+                                                             C.byref(ref)),
+                       "cfdb_simple_pprime_faces")
+        return f, bool(pin.value), int(ref.value)
 
     def iterate(self, n: int) -> SIMPLEResult:
         hist = np.zeros(5 * max(n, 1))

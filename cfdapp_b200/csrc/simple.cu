@@ -519,6 +519,18 @@ cfdb_status cfdb_simple_get_state(cfdb_simple* s, double* u, double* v, double* 
   return CFDB_OK;
 }
 
+cfdb_status cfdb_simple_pprime_faces(cfdb_simple* s, double* faces, int* pinned,
+                                     int64_t* reference_cell) {
+  if (!s || !faces) return CFDB_ERR_INVALID_ARGUMENT;
+  cfdb_context* ctx = s->ctx;
+  CFDB_CUDA(ctx, cudaMemcpyAsync(faces, s->D, sizeof(double) * (size_t)s->nf,
+                                 cudaMemcpyDeviceToHost, ctx->stream));
+  CFDB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (pinned) *pinned = s->pin ? 1 : 0;
+  if (reference_cell) *reference_cell = s->st.reference_cell;
+  return CFDB_OK;
+}
+
 cfdb_status cfdb_simple_pressure_gradient(cfdb_simple* s, double* gx, double* gy, double* gz) {
   if (!s || !gx || !gy) return CFDB_ERR_INVALID_ARGUMENT;
   gradient(s, s->d_ptype, s->d_pvalue, s->p, s->gradP);

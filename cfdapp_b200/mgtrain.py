@@ -7,10 +7,12 @@ network's own forward kernels and hand-written adjoint kernels); this script
 only draws the training problems, runs Adam on the few dozen weights, and
 keeps the weight set that needs the fewest flexible-CG iterations on the
 validation systems.  Training problems are p' operators of the kind the
-SIMPLE loop produces: the isolated (unit-response) operator and operators
-whose face coefficients follow smooth random log-normal response fields
-(the momentum response d = V / a_P varies smoothly across a flow), on
-grids small enough that one step takes milliseconds.  Error samples are
+SIMPLE loop produces: the isolated (unit-response) operator, operators whose
+face coefficients follow smooth random log-normal response fields (the
+momentum response d = V / a_P varies smoothly across a flow), and p' systems
+harvested from the library's own GPU SIMPLE runs of lid-driven cavities at
+Re 100, 400 and 1000 (cfdb_simple_pprime_faces), on grids small enough that
+one step takes milliseconds.  Error samples are
 multi-scale random fields (white noise at every level of the hierarchy,
 prolongated by injection), so smooth and rough error components are both
 represented; optionally some samples are replaced by the error fields the
@@ -127,6 +129,30 @@ def hard_errors(op, dim, n, fc, e0, sweeps=4):
     return np.array(out, dtype=np.float32)
 
 
+def harvest_cavity(ctx, dim, n, reynolds, snapshots, chunk=10):
+    """p' systems of the solver's own GPU SIMPLE runs: a lid-driven cavity at
+    each Reynolds number, the p' face coefficients taken every `chunk` outer
+    iterations until `snapshots` are collected.  Returns [(faces, pinned,
+    reference cell)]."""
+    out = []
+    for re in reynolds:
+        case = cfdb.SimpleCase.cavity(dim, n, lid=1.0, mu=1.0 / re)
+        ps = cfdb.LinearSolverSettings(absolute_tolerance=0.0, relative_tolerance=1e-8,
+                                       max_iterations=20000, type="cg",
+                                       preconditioner="learned_mg")
+        ms = cfdb.LinearSolverSettings(absolute_tolerance=1e-12, relative_tolerance=1e-8,
+                                       max_iterations=2000, type="bicgstab", preconditioner="none")
+        st = cfdb.SIMPLESettings(max_iterations=chunk * snapshots, momentum_solver=ms,
+                                 pressure_solver=ps)
+        sim = cfdb.Simple(ctx, case, st)
+        sim.set_state(None, None, None, None)
+        for _ in range(snapshots):
+            sim.iterate(chunk)
+            out.append(sim.pprime_faces())
+        sim.close()
+    return out
+
+
 def random_operator_faces(dim, n, rng):
     """Face coefficients (global real order) of a SIMPLE-like p' operator:
     D_f = interpolated smooth response d across each interior face, all-Neumann."""
@@ -214,15 +240,22 @@ def train_dim(ctx, dim, steps, seed, log, hard):
     n_train = (128, 128) if dim == 2 else (32, 32, 32)
     n_val = (384, 384) if dim == 2 else (64, 64, 64)
     nu, sweeps = 2, 50
-    # training operators: isolated + smooth-response variants
+    # training operators: isolated, smooth random response, and p' systems
+    # harvested from the solver's own SIMPLE runs of cavities at Re 100..1000
     train_fc = [uniform_faces(dim, n_train)] + [random_operator_faces(dim, n_train, rng)
-                                                for _ in range(3)]
+                                                for _ in range(2)]
+    harvested = harvest_cavity(ctx, dim, n_train[0], [100.0, 400.0, 1000.0], 2)
+    train_fc += [f for f, _, _ in harvested]
     train_ops = [cfdb.POperator(ctx, dim, n_train, face_coeff=fc) for fc in train_fc]
-    # validation: the isolated system and one smooth-response system, synthetic RHS
+    log(f"dim {dim}: {len(train_ops)} training operators ({len(harvested)} harvested)")
+    # validation: the isolated system, a smooth-response system and a
+    # harvested cavity system (Re 700), synthetic RHS
+    hv = harvest_cavity(ctx, dim, n_val[0], [700.0], 1, chunk=20)[0][0]
     val_ops = [cfdb.POperator(ctx, dim, n_val),
                cfdb.POperator(ctx, dim, n_val,
-                              face_coeff=random_operator_faces(dim, n_val, np.random.default_rng(seed + 99)))]
-    b_val = [cfdb.synth_rhs(dim, n_val[0])] * 2
+                              face_coeff=random_operator_faces(dim, n_val, np.random.default_rng(seed + 99))),
+               cfdb.POperator(ctx, dim, n_val, face_coeff=hv)]
+    b_val = [cfdb.synth_rhs(dim, n_val[0])] * 3
     ctx.mg_reset_weights(dim, trained=False)
     base = ctx.mg_get_weights(dim)
     k0 = np.repeat(base["kernels"][:1], TRAIN_LEVELS, axis=0)

@@ -253,6 +253,13 @@ CFDB_API cfdb_status cfdb_simple_solve(cfdb_context* ctx, const cfdb_simple_case
                                        double* w, double* p, double* flux, double* history,
                                        cfdb_simple_result* result);
 
+/* No counterpart in the reference.  The face coefficients D_f (global face
+ * order) of the p' system the session assembled last, with its pinning (1
+ * and the reference cell when no FixedValue pressure patch exists): the
+ * systems the learned preconditioner is trained and evaluated on. */
+CFDB_API cfdb_status cfdb_simple_pprime_faces(cfdb_simple* s, double* faces, int* pinned,
+                                             int64_t* reference_cell);
+
 /* Stage-level session (the reference's GpuSimpleDiscretization,
  * include/cfd/gpu/GpuSimpleDiscretization.hpp:56-262): upload a state, run
  * single stages or outer iterations, read results back. */
