@@ -69,9 +69,10 @@ def load() -> C.CDLL:
     global _lib
     if _lib is not None:
         return _lib
-    if not os.path.exists(LIB_PATH):
-        raise CfdbError(f"{LIB_PATH} is missing: build it with `python -m cfdapp_b200.build`")
-    L = C.CDLL(LIB_PATH)
+    path = os.environ.get("CFDB_LIBRARY") or LIB_PATH  # another build of the same library
+    if not os.path.exists(path):
+        raise CfdbError(f"{path} is missing: build it with `python -m cfdapp_b200.build`")
+    L = C.CDLL(path)
     vp, i64, dbl = C.c_void_p, C.c_int64, C.c_double
     L.cfdb_cuda_available.restype = C.c_int
     L.cfdb_create.argtypes = [C.c_int, vp, C.POINTER(vp)]

@@ -858,6 +858,120 @@ CoarsePlan coarse_plan(const MgHierarchy& H, const MgWeights& W) {
   return P;
 }
 
+// -------------------------------------------------- flat small-level passes
+//
+// Levels of at most kFlatCells cells are latency-bound: a plane march would
+// chain a few dependent load/barrier steps per block for almost no data.
+// These passes give every cell its own thread (all loads independent), so a
+// pass costs about one memory latency.
+constexpr int64_t kFlatCells = 1 << 16;
+
+__device__ __forceinline__ void cell_ijk(const LV& L, int64_t c, int& i, int& j, int& k) {
+  i = (int)(c % L.nx);
+  const int64_t rest = c / L.nx;
+  j = (int)(rest % L.ny);
+  k = (int)(rest / L.ny);
+}
+
+// res = r - A x (PRO: x + cw P ec in place of x), r[skip] read as 0
+template <int DIM, bool PRO>
+__global__ void __launch_bounds__(256) k_res_f(LV L, LV C, const float* __restrict__ x,
+                                               const float* __restrict__ ec, float cw,
+                                               const float* __restrict__ r, float* __restrict__ res,
+                                               int64_t skip) {
+  const int64_t n = (int64_t)L.nx * L.ny * L.nz;
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
+       c += (int64_t)gridDim.x * blockDim.x) {
+    int i, j, k;
+    cell_ijk(L, c, i, j, k);
+    const int64_t plane = (int64_t)L.nx * L.ny;
+    auto xv = [&](int64_t q, int ii, int jj, int kk) {
+      float v = x[q];
+      if (PRO) v += cw * ec[parent(C, ii, jj, kk)];
+      return v;
+    };
+    const float v = xv(c, i, j, k);
+    const float w = i > 0 ? xv(c - 1, i - 1, j, k) : 0.f;
+    const float e = i + 1 < L.nx ? xv(c + 1, i + 1, j, k) : 0.f;
+    const float s = (DIM == 3 && j > 0) ? xv(c - L.nx, i, j - 1, k) : 0.f;
+    const float nn = (DIM == 3 && j + 1 < L.ny) ? xv(c + L.nx, i, j + 1, k) : 0.f;
+    const float b = k > 0 ? xv(c - plane, i, j, k - 1) : 0.f;
+    const float t = k + 1 < L.nz ? xv(c + plane, i, j, k + 1) : 0.f;
+    res[c] = (c == skip ? 0.f : r[c]) - apply7(coef<DIM>(L, i, j, k), v, w, e, s, nn, b, t);
+  }
+}
+
+// rc(C) = sum of the children's (r - A x)
+template <int DIM>
+__global__ void __launch_bounds__(256) k_restrict_f(LV L, LV C, const float* __restrict__ x,
+                                                    const float* __restrict__ r,
+                                                    float* __restrict__ rc, int64_t skip) {
+  const int64_t n = (int64_t)C.nx * C.ny * C.nz;
+  for (int64_t qc = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; qc < n;
+       qc += (int64_t)gridDim.x * blockDim.x) {
+    int ci, cj, ck;
+    cell_ijk(C, qc, ci, cj, ck);
+    float sum = 0.f;
+    for (int u = 0; u < 2; ++u)
+      for (int v = 0; v < 2; ++v)
+        for (int t = 0; t < 2; ++t) {
+          const int i = 2 * ci + t, j = 2 * cj + v, k = 2 * ck + u;
+          if (i >= L.nx || j >= L.ny || k >= L.nz) continue;
+          const int64_t c = at(L, i, j, k);
+          const int64_t plane = (int64_t)L.nx * L.ny;
+          const float w = i > 0 ? x[c - 1] : 0.f, e = i + 1 < L.nx ? x[c + 1] : 0.f;
+          const float s = (DIM == 3 && j > 0) ? x[c - L.nx] : 0.f;
+          const float nn = (DIM == 3 && j + 1 < L.ny) ? x[c + L.nx] : 0.f;
+          const float b = k > 0 ? x[c - plane] : 0.f, tt = k + 1 < L.nz ? x[c + plane] : 0.f;
+          sum += (c == skip ? 0.f : r[c]) - apply7(coef<DIM>(L, i, j, k), x[c], w, e, s, nn, b, tt);
+        }
+    rc[qc] = sum;
+  }
+}
+
+// x <- [x] (+ cw P ec) + D^-1/2 (W * (D^-1/2 u)), u = res, or r (r[skip]
+// = 0) from x = 0 (FIRST); pin >= 0: x[pin] = r[pin]
+template <int DIM, int MODE>
+__global__ void __launch_bounds__(256) k_sm_f(LV L, LV C, Kern K, const float* __restrict__ src,
+                                              const float* __restrict__ ec, float cw,
+                                              float* __restrict__ x, int64_t skip, int64_t pin,
+                                              const float* __restrict__ r) {
+  const int64_t n = (int64_t)L.nx * L.ny * L.nz;
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
+       c += (int64_t)gridDim.x * blockDim.x) {
+    int i, j, k;
+    cell_ijk(L, c, i, j, k);
+    float sum = 0.f;
+#pragma unroll
+    for (int dk = -1; dk <= 1; ++dk) {
+      const int kk = k + dk;
+      if (kk < 0 || kk >= L.nz) continue;
+#pragma unroll
+      for (int dj = (DIM == 2 ? 0 : -1); dj <= (DIM == 2 ? 0 : 1); ++dj) {
+        const int jj = j + dj;
+        if (jj < 0 || jj >= L.ny) continue;
+#pragma unroll
+        for (int di = -1; di <= 1; ++di) {
+          const int ii = i + di;
+          if (ii < 0 || ii >= L.nx) continue;
+          const int64_t q = at(L, ii, jj, kk);
+          const float u = (MODE == SM_FIRST && q == skip) ? 0.f : src[q] * L.isq[q];
+          sum += K.w[(dk + 1) * 9 + (dj + 1) * 3 + (di + 1)] * u;
+        }
+      }
+    }
+    float v = L.isq[c] * sum;
+    if (MODE == SM_ADD) v += x[c];
+    if (ec) v += cw * ec[parent(C, i, j, k)];
+    if (c == pin) v = r[c];
+    x[c] = v;
+  }
+}
+
+int flat_blocks(int64_t n) {
+  return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 8));
+}
+
 #include "mg_quad.cuh"
 
 // Launchers of one level's passes, with the cells-per-thread choice.
@@ -892,7 +1006,17 @@ struct LevelOps {
 template <int DIM>
 void level_res(const MgLevel& M, const LV& LC, const float* x, const float* ec, float cw,
                const float* r, float* res, float* rc, int64_t skip, cudaStream_t st) {
-  if (quad_ok<DIM>(M.n[0])) {
+  if (M.cells <= kFlatCells) {
+    const LV L = lv(M);
+    if (rc) {
+      const int64_t nc = (int64_t)LC.nx * LC.ny * LC.nz;
+      k_restrict_f<DIM><<<flat_blocks(nc), 256, 0, st>>>(L, LC, x, r, rc, skip);
+    } else if (ec) {
+      k_res_f<DIM, true><<<flat_blocks(M.cells), 256, 0, st>>>(L, LC, x, ec, cw, r, res, skip);
+    } else {
+      k_res_f<DIM, false><<<flat_blocks(M.cells), 256, 0, st>>>(L, LC, x, ec, cw, r, res, skip);
+    }
+  } else if (quad_ok<DIM>(M.n[0])) {
     const Seg sg = make_quad_seg<DIM>(M.n[0], M.n[1], M.n[2]);
     const int g = quad_grid<DIM>(sg);
     constexpr int T = Quad<DIM>::TX * Quad<DIM>::TY;
@@ -909,7 +1033,13 @@ template <int DIM>
 void level_sm(const MgLevel& M, const LV& LC, const Kern& K, bool first, const float* src,
               const float* ec, float cw, float* x, int64_t skip, int64_t pin, const float* r,
               const Hook* hook, cudaStream_t st) {
-  if (quad_ok<DIM>(M.n[0])) {
+  if (M.cells <= kFlatCells && !hook) {
+    const LV L = lv(M);
+    if (first)
+      k_sm_f<DIM, SM_FIRST><<<flat_blocks(M.cells), 256, 0, st>>>(L, LC, K, src, ec, cw, x, skip, pin, r);
+    else
+      k_sm_f<DIM, SM_ADD><<<flat_blocks(M.cells), 256, 0, st>>>(L, LC, K, src, ec, cw, x, skip, pin, r);
+  } else if (quad_ok<DIM>(M.n[0])) {
     const Seg sg = make_quad_seg<DIM>(M.n[0], M.n[1], M.n[2]);
     const int g = quad_grid<DIM>(sg);
     constexpr int T = Quad<DIM>::TX * Quad<DIM>::TY;
