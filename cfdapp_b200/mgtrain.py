@@ -235,11 +235,10 @@ def fcg_iterations(ctx, ops, b_list):
     return its
 
 
-def train_dim(ctx, dim, steps, seed, log, hard):
+def train_dim(ctx, dim, steps, seed, log, hard, nu=2, sweeps=50):
     rng = np.random.default_rng(seed)
     n_train = (128, 128) if dim == 2 else (32, 32, 32)
     n_val = (384, 384) if dim == 2 else (64, 64, 64)
-    nu, sweeps = 2, 50
     # training operators: isolated, smooth random response, and p' systems
     # harvested from the solver's own SIMPLE runs of cavities at Re 100..1000
     train_fc = [uniform_faces(dim, n_train)] + [random_operator_faces(dim, n_train, rng)
@@ -355,6 +354,10 @@ def main():
     ap.add_argument("--dims", type=int, nargs="+", default=[2, 3])
     ap.add_argument("--steps", type=int, default=400)
     ap.add_argument("--seed", type=int, default=20261203)
+    ap.add_argument("--nu", type=int, nargs="+", default=[1, 1],
+                    help="smoothing layers per side, per dim (2D, 3D)")
+    ap.add_argument("--coarse-sweeps", type=int, nargs="+", default=[5, 20],
+                    help="damped-Jacobi sweeps on the coarsest level, per dim (2D, 3D)")
     ap.add_argument("--hard", type=int, nargs="+", default=[0, 2],
                     help="per dim (2D, 3D): samples of 4 drawn by power iteration of I - M A")
     ap.add_argument("--out", default=os.path.join(os.path.dirname(__file__), "csrc"))
@@ -364,7 +367,10 @@ def main():
     log = lambda s: print(f"[{time.time() - t0:7.1f}s] {s}", flush=True)
     sets = {}
     for dim in a.dims:
-        sets[dim] = train_dim(ctx, dim, a.steps, a.seed + dim, log, a.hard[0 if dim == 2 else 1])
+        q = 0 if dim == 2 else 1
+        pick = lambda v: v[q] if len(v) > q else v[-1]
+        sets[dim] = train_dim(ctx, dim, a.steps, a.seed + dim, log, pick(a.hard), pick(a.nu),
+                              pick(a.coarse_sweeps))
     digest = write_outputs(a.out, sets)
     log(f"wrote {a.out}/mg_trained.inc and mg_weights.json (sha256 {digest[:16]})")
     ctx.close()

@@ -238,17 +238,22 @@ def test_gradient_matches_finite_differences(ctx, dim, n):
 @pytest.mark.parametrize("dim,n,gain", [(2, 512, 0.8), (3, 96, 0.6)])
 def test_trained_weights_cut_iterations(ctx, dim, n, gain):
     """The shipped (GPU-trained) weights need clearly fewer FCG iterations
-    than the untrained network (damped Jacobi layers) on systems larger than
-    any seen in training (128^2 / 32^3): the isolated p' system and a
-    smooth-response one."""
+    than the untrained network (damped-Jacobi layers in the same cycle) on
+    systems larger than any seen in training (128^2 / 32^3): the isolated p'
+    system and a smooth-response one."""
     from cfdapp_b200.cfdb import POperator
     from cfdapp_b200.mgtrain import random_operator_faces
     b = O.synth_rhs(dim, n)
     ops = [POperator(ctx, dim, [n] * dim),
            POperator(ctx, dim, [n] * dim,
                      face_coeff=random_operator_faces(dim, [n] * dim, np.random.default_rng(5)))]
+    ctx.mg_reset_weights(dim, trained=True)
+    w = ctx.mg_get_weights(dim)
+    jacobi = np.zeros((1, 27), np.float32)
+    jacobi[0, 13] = 0.8  # the untrained layers: damped Jacobi, same cycle shape
     for op in ops:
-        ctx.mg_reset_weights(dim, trained=False)
+        ctx.mg_set_weights(dim, jacobi, np.ones(1, np.float32), nu=w["nu"],
+                           coarse_sweeps=w["coarse_sweeps"])
         untrained = op.solve(b, _settings())
         ctx.mg_reset_weights(dim, trained=True)
         trained = op.solve(b, _settings())
