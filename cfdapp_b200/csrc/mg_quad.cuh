@@ -350,7 +350,7 @@ __global__ void __launch_bounds__(Quad<DIM>::TX* Quad<DIM>::TY)
 
 // The quad counterpart of the FCG direction pass (see k_fcg_dir).
 template <int DIM>
-__global__ void __launch_bounds__(Quad<DIM>::TX* Quad<DIM>::TY, DIM == 3 ? 2 : 12)
+__global__ void __launch_bounds__(Quad<DIM>::TX* Quad<DIM>::TY, DIM == 3 ? 2 : 8)
     k_fcg_dir_q(OpView<double> A, Seg sg, FcgState* S, const float* __restrict__ z, double* P0,
                 double* P1, double* __restrict__ q, const double* __restrict__ r, double* partials,
                 Loop h) {
@@ -390,11 +390,48 @@ __global__ void __launch_bounds__(Quad<DIM>::TX* Quad<DIM>::TY, DIM == 3 ? 2 : 1
             const V4<double>& t) {
           if (!act) return;
           const int64_t c = idx(i0, j, k);
+          // couplings of the quad: per-face arrays or per-axis tables
+          double fx[5];
+          if (A.fx) {
+            const int64_t bx = i0 + (int64_t)(A.nx + 1) * (j + (int64_t)A.ny * k);
+#pragma unroll
+            for (int u = 0; u < 5; ++u) fx[u] = A.fx[bx + u];
+          } else {
+#pragma unroll
+            for (int u = 0; u < 5; ++u) fx[u] = A.tx[i0 + u];
+          }
+          V4<double> yl, yh, zl, zh;
+          if (A.fy) {
+            const int64_t by = i0 + (int64_t)A.nx * (j + (int64_t)(A.ny + 1) * k);
+            yl = ld4(A.fy + by);
+            yh = ld4(A.fy + by + A.nx);
+          } else {
+            const double a = A.ty[j], bb = A.ty[j + 1];
+            yl = V4<double>{{a, a, a, a}};
+            yh = V4<double>{{bb, bb, bb, bb}};
+          }
+          if (A.fz) {
+            zl = ld4(A.fz + c);
+            zh = ld4(A.fz + c + (int64_t)A.nx * A.ny);
+          } else {
+            const double a = A.tz[k], bb = A.tz[k + 1];
+            zl = V4<double>{{a, a, a, a}};
+            zh = V4<double>{{bb, bb, bb, bb}};
+          }
           V4<double> aq;
 #pragma unroll
-          for (int u = 0; u < 4; ++u)
-            aq.v[u] = apply_coef(load_coef(A, i0 + u, j, k), v.v[u], w.v[u], e.v[u], s.v[u],
-                                 n.v[u], b.v[u], t.v[u]);
+          for (int u = 0; u < 4; ++u) {
+            // diagonal summed in the reference's face order (as load_coef)
+            const double d =
+                ((((fx[u] + fx[u + 1]) + yl.v[u]) + yh.v[u]) + zl.v[u]) + zh.v[u];
+            double off = fx[u] * w.v[u];
+            off = fma(fx[u + 1], e.v[u], off);
+            off = fma(yl.v[u], s.v[u], off);
+            off = fma(yh.v[u], n.v[u], off);
+            off = fma(zl.v[u], b.v[u], off);
+            off = fma(zh.v[u], t.v[u], off);
+            aq.v[u] = (A.pinned && c + u == A.ref) ? v.v[u] : fma(d, v.v[u], -off);
+          }
           st4(pn + c, v);
           st4(q + c, aq);
           const V4<double> rr = ld4(r + c);
