@@ -44,6 +44,10 @@ def parse():
     ap.add_argument("--impl", default="cfdb", choices=["cfdb", "reference"])
     ap.add_argument("--grids", default=None, help="override, e.g. '2:512,3:64'")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="pprime", choices=["pprime", "batched"],
+                    help="pprime: the isolated p' solve (headline); batched: uneven "
+                         "cavity/channel SIMPLE cases advanced as one batch")
+    ap.add_argument("--cases", type=int, default=64)
     return ap.parse_args()
 
 
@@ -225,9 +229,196 @@ def _estimate_iterations(O, dim, n):
     return int(r.iterations * n / m)
 
 
+# ------------------------------------------------------------------ batched SIMPLE
+BATCH_SIDES = (64, 96, 128, 192, 256, 384, 512)
+BATCH_METRIC = "batched SIMPLE cell outer-iterations per second"
+
+
+def batched_cases(seed, ncases):
+    """Seeded uneven case list: side uniform in BATCH_SIDES, Re uniform in
+    [100, 1000], lid-driven cavity (unit square, lid 1) or channel (4 x 1,
+    side x side/4 cells, inlet 1 on the left, outlet on the right)."""
+    from cfdapp_b200.cfdb import SimpleCase
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(ncases):
+        side = int(rng.choice(BATCH_SIDES))
+        re = float(rng.uniform(100.0, 1000.0))
+        if rng.random() < 0.5:
+            out.append(("cavity", side, re, SimpleCase.cavity(2, side, mu=1.0 / re)))
+        else:
+            out.append(("channel", side, re,
+                        SimpleCase.channel(side, max(side // 4, 8), 4.0, 1.0, inlet=1.0,
+                                           mu=1.0 / re)))
+    return out
+
+
+def batched_settings():
+    from cfdapp_b200.cfdb import LinearSolverSettings, SIMPLESettings
+    return SIMPLESettings(
+        max_iterations=100000, velocity_relaxation=0.7, pressure_relaxation=0.3,
+        velocity_tolerance=1e-6, pressure_tolerance=1e-6, continuity_tolerance=1e-6,
+        convection_scheme="upwind", face_flux="linear",
+        momentum_solver=LinearSolverSettings(type="bicgstab", preconditioner="none",
+                                             absolute_tolerance=1e-10, relative_tolerance=1e-8,
+                                             max_iterations=500),
+        pressure_solver=LinearSolverSettings(type="cg", preconditioner="jacobi",
+                                             absolute_tolerance=0.0, relative_tolerance=1e-8,
+                                             max_iterations=20000))
+
+
+def batched_cpu_baseline(cases, outer=2):
+    """The reference's SIMPLE (oracle/_ref, OpenMP over the host's cores) on a
+    bounded sample: one case of each of three sides, `outer` outer iterations
+    each, in cell outer-iterations per second."""
+    from oracle import oracle as O
+    if not O.ref_driver_available():
+        return None
+    cores = os.cpu_count() or 1
+    env = dict(os.environ, OMP_NUM_THREADS=str(cores))
+    work, secs, picked = 0.0, 0.0, []
+    for side in (64, 128, 256):
+        c = next((c for c in cases if c[1] == side), None)
+        if c is None:
+            continue
+        kind, _, re, case = c
+        args = [O.REF_DRIVER, "simple", "dim=2", f"outer={outer}", f"mu={1.0 / re!r}",
+                "flux=linear", "tolu=1e-6", "tolp=1e-6", "tolc=1e-6", "pmax=20000"]
+        if kind == "cavity":
+            args += [f"nx={side}", f"ny={side}"]
+        else:
+            args += ["flow=channel", f"nx={side}", f"ny={max(side // 4, 8)}", "lx=4", "ly=1"]
+        out = subprocess.run(args, capture_output=True, text=True, env=env, check=True)
+        d = json.loads(out.stdout)
+        work += d["cells"] * d["iterations"]
+        secs += d["seconds"]
+        picked.append(f"{kind} {case.n[0]}x{case.n[1]} Re {re:.0f}: {d['iterations']} outer "
+                      f"iterations in {d['seconds']:.2f} s")
+    if secs <= 0:
+        return None
+    return {"value": work / secs, "unit": "cell outer-iterations/s", "cores": cores,
+            "kind": "reference", "sample": "; ".join(picked)}
+
+
+def run_batched(a):
+    from cfdapp_b200 import cfdb
+    rank, world, local = dist_info()
+    torch_dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+        torch_dist = dist
+    if not cfdb.cuda_available():
+        raise SystemExit("bench.py: no sm_100 device visible (the product has no CPU path)")
+    ctx = cfdb.Context(local)
+    cases = batched_cases(SEED + rank, a.cases)
+    s = batched_settings()
+    b = cfdb.Batch(ctx, [c[3] for c in cases], s)
+    for k in range(len(cases)):
+        b.set_state(k)
+    cells = np.array([c[3].cells() for c in cases], dtype=np.float64)
+
+    def counters():
+        r = b.results()
+        return (np.array([x["iterations"] for x in r]),
+                np.array([x["pressure_linear_iterations"] for x in r]))
+
+    t0 = time.perf_counter()
+    tuning = b.autotune()
+    tune_s = time.perf_counter() - t0
+    b.iterate(a.warmup)
+    # one eager iteration with events around every launch: per-stage times and
+    # the p' solve kernel's roofline
+    _, p_before = counters()
+    prof = b.profile_iteration()
+    it0, p_after = counters()
+    p_ms = sum(ms for i, ms in prof if i == -2)
+    # algorithmic bytes of a Jacobi-CG iteration per cell: 14 + 2d FP64 words
+    # (p update 4, A p 3 + 2d, x and r update 7), d = 2
+    p_bytes = float(((p_after - p_before) * cells).sum()) * (14 + 2 * 2) * 8
+    peak, peak_kind = measured_peaks()
+    achieved = p_bytes / (p_ms * 1e-3) / 1e9 if p_ms > 0 else None
+    if torch_dist:
+        torch_dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    launches0 = ctx.launches()
+    st = b.iterate(a.steps)
+    clk = clocks.stop()
+    launches = ctx.launches() - launches0
+    it1, _ = counters()
+    work = float(((it1 - it0) * cells).sum())
+    dev_ms = st["device_ms"]
+    if torch_dist:
+        import torch
+        t = torch.tensor([dev_ms], device=f"cuda:{local}", dtype=torch.float64)
+        torch_dist.all_reduce(t, op=torch_dist.ReduceOp.MAX)
+        w = torch.tensor([work], device=f"cuda:{local}", dtype=torch.float64)
+        torch_dist.all_reduce(w, op=torch_dist.ReduceOp.SUM)
+        dev_ms, work = float(t.item()), float(w.item())
+    value = work / (dev_ms * 1e-3) if dev_ms > 0 else 0.0
+    # e2e through the public API: upload every case's state from host arrays,
+    # run the steps, download every case's fields
+    states = [b.get_state(k) for k in range(len(cases))]
+    h2d = d2h = 0
+    t0 = time.perf_counter()
+    for k, (u, v, _, p_, _) in enumerate(states):
+        b.set_state(k, u, v, None, p_)
+        h2d += u.nbytes + v.nbytes + p_.nbytes
+    b.iterate(a.steps)
+    for k in range(len(cases)):
+        u, v, _, p_, f = b.get_state(k)
+        d2h += u.nbytes + v.nbytes + p_.nbytes + f.nbytes
+    e2e_ms = (time.perf_counter() - t0) * 1e3
+    it2, _ = counters()   # set_state restarted every count at 0
+    e2e_work = float((it2 * cells).sum())
+    base = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        base = batched_cpu_baseline(cases)
+    if rank == 0:
+        stage_ms = {}
+        for i, ms in prof:
+            key = {-1: "momentum_solve", -2: "pprime_solve"}.get(i, f"stage_{i}")
+            stage_ms[key] = stage_ms.get(key, 0.0) + ms
+        line = {
+            "metric": BATCH_METRIC, "value": value, "unit": "cell outer-iterations/s",
+            "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": dev_ms / max(a.steps, 1), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"{len(cases)} uneven 2D SIMPLE cases per GPU (sides "
+                                   f"{list(BATCH_SIDES)}, Re 100-1000, cavity or channel, "
+                                   "seeded), upwind, linear flux, BiCGSTAB momentum, "
+                                   "Jacobi-PCG p' to 1e-8; one step = one outer iteration of "
+                                   "the whole batch (one CUDA graph launch)",
+                       "cells": int(cells.sum()), "l2": "inputs larger than L2",
+                       "parallelism": f"independent batches x{world}"},
+            "tuning": tuning.__dict__, "autotune_s": tune_s,
+            "profiled_iteration_ms": stage_ms,
+            "roofline": {"bound": "hbm", "kernel": "batched p' Jacobi-CG team kernel",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak if achieved else None,
+                         "peak_source": f"{peak_kind} hbm_gbs", "traffic": None},
+            "e2e": {"value": e2e_work / (e2e_ms * 1e-3), "unit": "cell outer-iterations/s",
+                    "h2d_bytes_per_step": h2d // max(a.steps, 1),
+                    "d2h_bytes_per_step": d2h // max(a.steps, 1)},
+            "gpu_launches": launches, "clocks": clk, "cpu_baseline": base,
+            "active_cases": st["active"],
+        }
+        print(json.dumps(line), flush=True)
+    b.close()
+    ctx.close()
+    if torch_dist:
+        torch_dist.destroy_process_group()
+    return 0
+
+
 # ------------------------------------------------------------------ device arm
 def main():
     a = parse()
+    if a.workload == "batched":
+        return run_batched(a)
     grids = grids_from(a)
     if a.impl == "reference":
         return run_reference(a, grids)

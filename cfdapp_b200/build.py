@@ -26,8 +26,9 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr", "--e
               "-Xcompiler", "-fPIC", "-Xcompiler", "-O2", "-Xcompiler", "-fvisibility=hidden"]
 # The SIMPLE stage kernels restate the reference's arithmetic operation by
 # operation; they are compiled without FMA contraction so that a stage
-# reproduces the reference bit for bit (the solvers keep FMA).
-PER_FILE_FLAGS = {"simple_kernels.cu": ["-fmad=false"]}
+# reproduces the reference bit for bit (the solvers keep FMA); the batched
+# stage kernels share their per-item code and are compiled the same way.
+PER_FILE_FLAGS = {"simple_kernels.cu": ["-fmad=false"], "batch_stages.cu": ["-fmad=false"]}
 
 
 def nvcc() -> str:

@@ -655,3 +655,202 @@ class Simple:
             self.close()
         except Exception:
             pass
+
+
+# ------------------------------------------------------------ batched SIMPLE
+class _BatchTuning(C.Structure):
+    _fields_ = [("cell_threads", C.c_int), ("cell_tile", C.c_int), ("face_threads", C.c_int),
+                ("face_tile", C.c_int), ("team_exponent", C.c_double),
+                ("adaptive_teams", C.c_int), ("cell_stage_ms", C.c_double),
+                ("face_stage_ms", C.c_double), ("pprime_solve_ms", C.c_double),
+                ("candidates", C.c_int)]
+
+
+class _BatchStats(C.Structure):
+    _fields_ = [("graph_launches", C.c_int64), ("active", C.c_int), ("device_ms", C.c_double),
+                ("kernel_launches", C.c_int64)]
+
+
+def _batch_sigs(L):
+    vp, i64 = C.c_void_p, C.c_int64
+    dp = C.POINTER(C.c_double)
+    ip = C.POINTER(C.c_int)
+    lp = C.POINTER(C.c_int64)
+    _simple_sigs(L)
+    L.cfdb_batch_create.argtypes = [vp, C.c_int, C.POINTER(_SimpleCase), C.POINTER(_SimpleSettings),
+                                    i64, C.POINTER(vp)]
+    L.cfdb_batch_destroy.argtypes = [vp]
+    L.cfdb_batch_destroy.restype = None
+    L.cfdb_batch_cases.argtypes = [vp]
+    L.cfdb_batch_set_state.argtypes = [vp, C.c_int, dp, dp, dp, dp]
+    L.cfdb_batch_get_state.argtypes = [vp, C.c_int, dp, dp, dp, dp, dp]
+    L.cfdb_batch_autotune.argtypes = [vp, C.POINTER(_BatchTuning)]
+    L.cfdb_batch_set_tuning.argtypes = [vp, C.POINTER(_BatchTuning)]
+    L.cfdb_batch_get_tuning.argtypes = [vp, C.POINTER(_BatchTuning)]
+    L.cfdb_batch_iterate.argtypes = [vp, i64, C.POINTER(_BatchStats)]
+    L.cfdb_batch_profile_iteration.argtypes = [vp, ip, dp, C.c_int, ip]
+    L.cfdb_batch_results.argtypes = [vp, C.POINTER(_SimpleResult)]
+    L.cfdb_batch_history.argtypes = [vp, C.c_int, dp, i64, lp]
+    L.cfdb_batch_plan_tiles.argtypes = [C.c_int, lp, C.c_int, ip, ip, lp]
+    L.cfdb_batch_plan_teams.argtypes = [C.c_int, dp, lp, ip, C.c_int, i64, ip, ip]
+
+
+def plan_tiles(counts, tile: int, lib=None):
+    """Tile list of the batch's stage kernels (host only): (first, tile_case, tile_start)."""
+    L = lib or load()
+    _batch_sigs(L)
+    cnt = np.ascontiguousarray(counts, dtype=np.int64)
+    n = cnt.size
+    first = np.zeros(n + 1, dtype=np.int32)
+    ip, lp = C.POINTER(C.c_int), C.POINTER(C.c_int64)
+    st = L.cfdb_batch_plan_tiles(n, cnt.ctypes.data_as(lp), tile, first.ctypes.data_as(ip), None, None)
+    if st != 0:
+        raise CfdbError(f"cfdb_batch_plan_tiles failed ({st})")
+    tc = np.zeros(int(first[-1]), dtype=np.int32)
+    ts = np.zeros(int(first[-1]), dtype=np.int64)
+    st = L.cfdb_batch_plan_tiles(n, cnt.ctypes.data_as(lp), tile, first.ctypes.data_as(ip),
+                                 tc.ctypes.data_as(ip), ts.ctypes.data_as(lp))
+    if st != 0:
+        raise CfdbError(f"cfdb_batch_plan_tiles failed ({st})")
+    return first, tc, ts
+
+
+def plan_teams(weight, cells, active, nblocks: int, min_cells_per_block: int = 2048, lib=None):
+    """Krylov team table of the batch (host only): (team_first, block_case)."""
+    L = lib or load()
+    _batch_sigs(L)
+    w = np.ascontiguousarray(weight, dtype=np.float64)
+    c = np.ascontiguousarray(cells, dtype=np.int64)
+    a = np.ascontiguousarray(active, dtype=np.int32)
+    n = w.size
+    tf = np.zeros(n + 1, dtype=np.int32)
+    bc = np.zeros(nblocks, dtype=np.int32)
+    ip = C.POINTER(C.c_int)
+    st = L.cfdb_batch_plan_teams(n, w.ctypes.data_as(C.POINTER(C.c_double)),
+                                 c.ctypes.data_as(C.POINTER(C.c_int64)), a.ctypes.data_as(ip),
+                                 nblocks, min_cells_per_block, tf.ctypes.data_as(ip),
+                                 bc.ctypes.data_as(ip))
+    if st != 0:
+        raise CfdbError(f"cfdb_batch_plan_teams failed ({st})")
+    return tf, bc
+
+
+@dataclass
+class BatchTuning:
+    cell_threads: int = 256
+    cell_tile: int = 1024
+    face_threads: int = 256
+    face_tile: int = 1024
+    team_exponent: float = 1.5
+    adaptive_teams: bool = True
+    cell_stage_ms: float = 0.0
+    face_stage_ms: float = 0.0
+    pprime_solve_ms: float = 0.0
+    candidates: int = 0
+
+    @staticmethod
+    def of(t: _BatchTuning) -> "BatchTuning":
+        return BatchTuning(t.cell_threads, t.cell_tile, t.face_threads, t.face_tile,
+                           t.team_exponent, bool(t.adaptive_teams), t.cell_stage_ms,
+                           t.face_stage_ms, t.pprime_solve_ms, t.candidates)
+
+    def c(self) -> _BatchTuning:
+        return _BatchTuning(self.cell_threads, self.cell_tile, self.face_threads, self.face_tile,
+                            self.team_exponent, int(self.adaptive_teams), self.cell_stage_ms,
+                            self.face_stage_ms, self.pprime_solve_ms, self.candidates)
+
+
+class Batch:
+    """Many independent SIMPLE cases of one dimension advanced together (cfdb_batch_*)."""
+
+    def __init__(self, ctx: Context, cases, settings: SIMPLESettings, history_cap: int = 0):
+        self.ctx, self.cases, self.settings = ctx, list(cases), settings
+        self.history_cap = history_cap
+        _batch_sigs(ctx.lib)
+        arr = (_SimpleCase * len(self.cases))(*[c.c() for c in self.cases])
+        h = C.c_void_p()
+        ctx.check(ctx.lib.cfdb_batch_create(ctx.handle, len(self.cases), arr, C.byref(settings.c()),
+                                            history_cap, C.byref(h)), "cfdb_batch_create")
+        self._h = h
+
+    def set_state(self, k: int, u=None, v=None, w=None, p=None):
+        n = self.cases[k].cells()
+        arr = [np.ascontiguousarray(a if a is not None else np.zeros(n), dtype=np.float64)
+               for a in (u, v, w, p)]
+        self.ctx.check(self.ctx.lib.cfdb_batch_set_state(self._h, k, *[_dp(a) for a in arr]),
+                       "cfdb_batch_set_state")
+
+    def get_state(self, k: int):
+        case = self.cases[k]
+        n = case.cells()
+        u, v, w, p = (np.zeros(n) for _ in range(4))
+        f = np.zeros(case.faces())
+        self.ctx.check(self.ctx.lib.cfdb_batch_get_state(self._h, k, _dp(u), _dp(v), _dp(w), _dp(p),
+                                                         _dp(f)), "cfdb_batch_get_state")
+        return u, v, (w if case.dim == 3 else np.zeros(0)), p, f
+
+    def autotune(self) -> BatchTuning:
+        t = _BatchTuning()
+        self.ctx.check(self.ctx.lib.cfdb_batch_autotune(self._h, C.byref(t)), "cfdb_batch_autotune")
+        return BatchTuning.of(t)
+
+    @property
+    def tuning(self) -> BatchTuning:
+        t = _BatchTuning()
+        self.ctx.check(self.ctx.lib.cfdb_batch_get_tuning(self._h, C.byref(t)), "cfdb_batch_get_tuning")
+        return BatchTuning.of(t)
+
+    @tuning.setter
+    def tuning(self, t: BatchTuning):
+        self.ctx.check(self.ctx.lib.cfdb_batch_set_tuning(self._h, C.byref(t.c())),
+                       "cfdb_batch_set_tuning")
+
+    def iterate(self, n: int) -> dict:
+        s = _BatchStats()
+        self.ctx.check(self.ctx.lib.cfdb_batch_iterate(self._h, n, C.byref(s)), "cfdb_batch_iterate")
+        return dict(graph_launches=s.graph_launches, active=s.active, device_ms=s.device_ms,
+                    kernel_launches=s.kernel_launches)
+
+    def profile_iteration(self) -> list:
+        """One eager outer iteration with events around every launch: [(id, ms)];
+        id: stage number, -1 momentum solve kernel, -2 p' solve kernel."""
+        cap = 256
+        ids = np.zeros(cap, dtype=np.int32)
+        ms = np.zeros(cap)
+        cnt = C.c_int()
+        self.ctx.check(self.ctx.lib.cfdb_batch_profile_iteration(
+            self._h, ids.ctypes.data_as(C.POINTER(C.c_int)), _dp(ms), cap, C.byref(cnt)),
+            "cfdb_batch_profile_iteration")
+        n = min(cnt.value, cap)
+        return list(zip(ids[:n].tolist(), ms[:n].tolist()))
+
+    def results(self) -> list:
+        rs = (_SimpleResult * len(self.cases))()
+        self.ctx.check(self.ctx.lib.cfdb_batch_results(self._h, rs), "cfdb_batch_results")
+        out = []
+        for r in rs:
+            final = dict(u=r.final_u, v=r.final_v, w=r.final_w, p=r.final_p,
+                         continuity=r.final_continuity, global_imbalance=r.global_imbalance)
+            out.append(dict(status=SIMPLE_STATUS[r.status], iterations=r.iterations, final=final,
+                            momentum_linear_iterations=r.momentum_linear_iterations,
+                            pressure_linear_iterations=r.pressure_linear_iterations))
+        return out
+
+    def history(self, k: int) -> np.ndarray:
+        cap = max(self.history_cap, 1)
+        h = np.zeros(5 * cap)
+        rows = C.c_int64()
+        self.ctx.check(self.ctx.lib.cfdb_batch_history(self._h, k, _dp(h), cap, C.byref(rows)),
+                       "cfdb_batch_history")
+        return h[: 5 * rows.value].reshape(-1, 5)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.ctx.lib.cfdb_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

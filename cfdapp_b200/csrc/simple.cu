@@ -417,6 +417,15 @@ cfdb_status outer_iteration(cfdb_simple* s, int64_t it, double* hist, cfdb_simpl
 
 }  // namespace
 
+namespace cfdb {
+SGeo simple_geometry(const cfdb_simple_case& cs) { return make_geo(cs); }
+bool simple_wall_offsets(const SGeo& G) { return wall_offsets_nonzero(G); }
+cfdb_status simple_validate(cfdb_context* ctx, const cfdb_simple_case* cs,
+                            const cfdb_simple_settings* st) {
+  return validate(ctx, cs, st);
+}
+}  // namespace cfdb
+
 extern "C" {
 
 cfdb_status cfdb_simple_create(cfdb_context* ctx, const cfdb_simple_case* cs,

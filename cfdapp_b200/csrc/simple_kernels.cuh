@@ -5,6 +5,7 @@
 
 #include <cstdint>
 
+#include "cfdb.h"
 #include "simple_geo.cuh"
 
 namespace cfdb {
@@ -36,5 +37,11 @@ void launch_flux_correct(const SGeo& G, const double* Fs, const double* D, const
 int residual_sums_blocks(const SGeo& G);
 void launch_residual_sums(const SGeo& G, const double* F, double* partials, cudaStream_t s);
 void launch_nonfinite(int64_t n, const double* v, unsigned* flag, cudaStream_t s);
+
+// Host helpers of the single-case session (simple.cu), shared with the batch.
+SGeo simple_geometry(const cfdb_simple_case& cs);
+bool simple_wall_offsets(const SGeo& G);  // the wall stencil needs velocity gradients
+cfdb_status simple_validate(cfdb_context* ctx, const cfdb_simple_case* cs,
+                            const cfdb_simple_settings* st);
 
 }  // namespace cfdb

@@ -283,6 +283,101 @@ CFDB_API cfdb_status cfdb_simple_assemble_momentum(cfdb_simple* s, int comp, dou
 CFDB_API cfdb_status cfdb_simple_iterate(cfdb_simple* s, int64_t n, double* history,
                                          cfdb_simple_result* result);
 
+/* ---------------------------------------------------------- batched SIMPLE */
+
+/* No counterpart in the reference, which solves one case per process
+ * (ProjectRunner.cpp:278-282).  A batch advances many independent cases of
+ * one dimension and uneven size together on one GPU, all under one settings
+ * record: each SIMPLE stage is one persistent kernel over a tile list of all
+ * cases, each momentum and p' solve one kernel in which every case's
+ * Krylov solve runs on its own team of blocks, and one outer iteration of
+ * the whole batch is one CUDA graph launch.  Each case stops on its own
+ * (converged or failed) and keeps its state; the others go on.  Per case the
+ * stages, statuses and convergence test are those of cfdb_simple_iterate.
+ * Supported: FP64 linear solves, CG or BiCGSTAB, no or Jacobi
+ * preconditioning (others return CFDB_ERR_UNSUPPORTED). */
+typedef struct cfdb_batch cfdb_batch;
+
+/* Launch shapes of the batch: cells (faces) per tile and threads per block
+ * of the cell (face) stage kernels; the p' team sizes of the first outer
+ * iteration are proportional to cells^team_exponent, and with adaptive_teams
+ * every later iteration sizes them by cells x the case's last p' iteration
+ * count.  The autotuner fills the *_ms fields with the best times it
+ * measured (device time of one launch; 0 when not tuned). */
+typedef struct {
+  int cell_threads, cell_tile;
+  int face_threads, face_tile;
+  double team_exponent;
+  int adaptive_teams;
+  double cell_stage_ms, face_stage_ms, pprime_solve_ms;
+  int candidates;
+} cfdb_batch_tuning;
+
+typedef struct {
+  int64_t graph_launches;   /* outer iterations of the batch run by this call */
+  int active;               /* cases still iterating */
+  double device_ms;         /* summed device time of the launches (CUDA events) */
+  int64_t kernel_launches;  /* kernels those launches ran */
+} cfdb_batch_stats;
+
+/* cases[ncases], one dimension; history_cap > 0 keeps the first history_cap
+ * rows of every case's residual history ({u, v, w, p, continuity} per outer
+ * iteration, as cfdb_simple_solve writes it).  Initial state: zero fields. */
+CFDB_API cfdb_status cfdb_batch_create(cfdb_context* ctx, int ncases, const cfdb_simple_case* cases,
+                                       const cfdb_simple_settings* settings, int64_t history_cap,
+                                       cfdb_batch** out);
+CFDB_API void cfdb_batch_destroy(cfdb_batch* b);
+CFDB_API int cfdb_batch_cases(const cfdb_batch* b);
+/* Uploads case k's u, v, w (3D), p, computes its face flux from u and
+ * restarts its outer-iteration count (as cfdb_simple_set_state); a
+ * non-finite field stops the case at once with CFDB_SIMPLE_NONFINITE_STATE
+ * (the initial check of cfdb_simple_solve). */
+CFDB_API cfdb_status cfdb_batch_set_state(cfdb_batch* b, int k, const double* u, const double* v,
+                                          const double* w, const double* p);
+CFDB_API cfdb_status cfdb_batch_get_state(cfdb_batch* b, int k, double* u, double* v, double* w,
+                                          double* p, double* flux);
+/* Times candidate launch shapes on the batch's current state and keeps the
+ * fastest: stage tile and block sizes on the momentum-assembly and mass-flux
+ * stages, p' team sizing on the p' solves of the current state.  The state,
+ * statuses and counters are left as they were. */
+CFDB_API cfdb_status cfdb_batch_autotune(cfdb_batch* b, cfdb_batch_tuning* chosen);
+CFDB_API cfdb_status cfdb_batch_set_tuning(cfdb_batch* b, const cfdb_batch_tuning* t);
+CFDB_API cfdb_status cfdb_batch_get_tuning(cfdb_batch* b, cfdb_batch_tuning* t);
+/* Up to n outer iterations of every case still iterating (fewer if all stop). */
+CFDB_API cfdb_status cfdb_batch_iterate(cfdb_batch* b, int64_t n, cfdb_batch_stats* stats);
+/* One outer iteration run eagerly (not as a graph) with CUDA events around
+ * every launch, for profiling: ids[i] is the launch's stage (an internal
+ * stage number, -1 for a momentum solve kernel, -2 for the p' solve kernel)
+ * and ms[i] its device time; *count = launches (at most cap are written).
+ * The iteration is a real one: it advances the state like cfdb_batch_iterate. */
+CFDB_API cfdb_status cfdb_batch_profile_iteration(cfdb_batch* b, int* ids, double* ms, int cap,
+                                                  int* count);
+/* Per-case outcome (results[ncases]): status (CFDB_SIMPLE_MAX_ITERATIONS
+ * while a case still iterates), outer iterations, residuals of its last
+ * completed iteration, linear-iteration totals (timings are left 0). */
+CFDB_API cfdb_status cfdb_batch_results(cfdb_batch* b, cfdb_simple_result* results);
+/* Case k's residual history: up to cap rows of 5 doubles; *rows = rows kept. */
+CFDB_API cfdb_status cfdb_batch_history(cfdb_batch* b, int k, double* history, int64_t cap,
+                                        int64_t* rows);
+
+/* Host-only planning of the batch's work lists (no device needed).
+ * Tiles: case k's count[k] items split into ceil(count[k]/tile) tiles;
+ * first[ncases+1] is the prefix sum; tile_case/tile_start (may be NULL)
+ * receive each tile's case and first item. */
+CFDB_API cfdb_status cfdb_batch_plan_tiles(int ncases, const int64_t* count, int tile, int* first,
+                                           int* tile_case, int64_t* tile_start);
+/* Teams: nblocks blocks split among the active cases, each active case at
+ * least one block and at most max(1, cells[k] / min_cells_per_block);
+ * blocks go one at a time to the case with the most weight per block
+ * (highest weight[k] / blocks[k], lowest k on ties), which minimises the
+ * largest weight per block.  team_first[ncases+1] is the prefix sum (0
+ * blocks for inactive cases); block_case[nblocks] the case of each block
+ * (-1: idle).  CFDB_ERR_UNSUPPORTED if more cases are active than blocks. */
+CFDB_API cfdb_status cfdb_batch_plan_teams(int ncases, const double* weight, const int64_t* cells,
+                                           const int* active, int nblocks,
+                                           int64_t min_cells_per_block, int* team_first,
+                                           int* block_case);
+
 /* ------------------------------------------- learned preconditioner weights */
 
 /* No counterpart in the reference.  Weights of the CFDB_PRECOND_LEARNED_MG
