@@ -547,7 +547,8 @@ cfdb_status cfdb_batch_create(cfdb_context* ctx, int ncases, const cfdb_simple_c
     if (rc != CFDB_OK) return rc;
     if (cases[k].grid.dim != dim) return set_error(ctx, CFDB_ERR_INVALID_ARGUMENT, "a batch holds one dimension");
   }
-  if (!(st->alpha_u > 0.0) || st->alpha_u > 1.0 || !(st->alpha_p > 0.0) || st->alpha_p > 1.0 ||
+  if (st->max_outer < 1 || !(st->alpha_u > 0.0) || st->alpha_u > 1.0 || !(st->alpha_p > 0.0) ||
+      st->alpha_p > 1.0 ||
       st->momentum.max_iterations < 1 || st->pressure.max_iterations < 1)
     return set_error(ctx, CFDB_ERR_INVALID_ARGUMENT, "invalid relaxation or iteration limits");
   for (const cfdb_linear_settings* L : {&st->momentum, &st->pressure}) {
@@ -630,6 +631,7 @@ cfdb_status cfdb_batch_create(cfdb_context* ctx, int ncases, const cfdb_simple_c
     return rc;
   if (history_cap > 0 && (rc = dalloc(b.get(), &D.history, (size_t)ncases * history_cap * 5))) return rc;
   D.history_cap = history_cap;
+  D.max_outer = st->max_outer;
   D.alpha_u = st->alpha_u;
   D.alpha_p = st->alpha_p;
   D.tol_u = st->tol_u;

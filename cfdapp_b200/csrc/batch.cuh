@@ -94,6 +94,7 @@ struct BatchDev {
   int* nactive;       // active cases after the last outer iteration
   double* history;    // optional: 5 doubles per case per outer iteration
   int64_t history_cap;
+  int64_t max_outer;  // outer iterations after which a case stops (MAX_ITERATIONS)
   // settings shared by the batch
   double alpha_u, alpha_p, tol_u, tol_p, tol_c;
   int scheme, face_flux;

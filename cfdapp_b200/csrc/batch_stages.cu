@@ -11,8 +11,9 @@
 // atomic ticket): BS_CHECK_PP stops the cases whose p' is not finite, and
 // BS_RESIDUAL sums each case's continuity and net-flux partials in tile
 // order (deterministic), stops cases with non-finite fields, makes the
-// corrected flux current, counts the outer iteration and applies the
-// convergence test (SolverRobustness.cpp:361-372 through SIMPLE.cpp:1025-1103).
+// corrected flux current, counts the outer iteration, applies the
+// convergence test (SolverRobustness.cpp:361-372 through SIMPLE.cpp:1025-1103)
+// and stops a case at the settings' outer-iteration limit.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -329,6 +330,9 @@ __global__ void k_residual(BatchDev B) {
                         (K.G.dim == 2 || R[BR_W] <= B.tol_u);
       if (conv) {
         B.status[k] = CFDB_SIMPLE_CONVERGED;
+        B.active[k] = 0;
+      } else if (it + 1 >= B.max_outer) {
+        B.status[k] = CFDB_SIMPLE_MAX_ITERATIONS;
         B.active[k] = 0;
       }
     }

@@ -343,7 +343,9 @@ CFDB_API cfdb_status cfdb_batch_get_state(cfdb_batch* b, int k, double* u, doubl
 CFDB_API cfdb_status cfdb_batch_autotune(cfdb_batch* b, cfdb_batch_tuning* chosen);
 CFDB_API cfdb_status cfdb_batch_set_tuning(cfdb_batch* b, const cfdb_batch_tuning* t);
 CFDB_API cfdb_status cfdb_batch_get_tuning(cfdb_batch* b, cfdb_batch_tuning* t);
-/* Up to n outer iterations of every case still iterating (fewer if all stop). */
+/* Up to n outer iterations of every case still iterating (fewer if all stop);
+ * a case stops at convergence, on failure, or after settings->max_outer
+ * outer iterations in all (status CFDB_SIMPLE_MAX_ITERATIONS). */
 CFDB_API cfdb_status cfdb_batch_iterate(cfdb_batch* b, int64_t n, cfdb_batch_stats* stats);
 /* One outer iteration run eagerly (not as a graph) with CUDA events around
  * every launch, for profiling: ids[i] is the launch's stage (an internal
