@@ -44,9 +44,11 @@ def parse():
     ap.add_argument("--impl", default="cfdb", choices=["cfdb", "reference"])
     ap.add_argument("--grids", default=None, help="override, e.g. '2:512,3:64'")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="pprime", choices=["pprime", "batched"],
+    ap.add_argument("--workload", default="pprime", choices=["pprime", "batched", "cavity3d"],
                     help="pprime: the isolated p' solve (headline); batched: uneven "
-                         "cavity/channel SIMPLE cases advanced as one batch")
+                         "cavity/channel SIMPLE cases advanced as one batch; cavity3d: outer "
+                         "iterations of the 256^3 Re-1000 lid-driven cavity")
+    ap.add_argument("--n3d", type=int, default=256)
     ap.add_argument("--cases", type=int, default=64)
     return ap.parse_args()
 
@@ -414,11 +416,88 @@ def run_batched(a):
     return 0
 
 
+# ------------------------------------------------------------------ 3D cavity SIMPLE
+CAVITY3D_METRIC = "3D cavity SIMPLE ms per outer iteration"
+
+
+def cavity3d_settings(pressure: str):
+    from cfdapp_b200.cfdb import LinearSolverSettings, SIMPLESettings
+    pre = "learned_mg" if pressure == "learned" else "jacobi"
+    return SIMPLESettings(
+        max_iterations=100000, velocity_relaxation=0.7, pressure_relaxation=0.3,
+        velocity_tolerance=1e-6, pressure_tolerance=1e-6, continuity_tolerance=1e-6,
+        convection_scheme="linear_upwind", face_flux="rhie_chow",
+        momentum_solver=LinearSolverSettings(type="bicgstab", preconditioner="none",
+                                             absolute_tolerance=1e-10, relative_tolerance=1e-8,
+                                             max_iterations=500),
+        pressure_solver=LinearSolverSettings(type="cg", preconditioner=pre,
+                                             absolute_tolerance=0.0, relative_tolerance=1e-8,
+                                             max_iterations=200000))
+
+
+def run_cavity3d(a):
+    """Outer iterations of the n^3 lid-driven cavity at Re 1000 (rho 1, mu
+    1e-3, lid 1), linear-upwind deferred correction, Rhie-Chow flux, every p'
+    system solved by the learned-FCG to 1e-8; the FP64 Jacobi-PCG p' solve of
+    the same state is timed beside it for one iteration.  One step = one
+    outer iteration; value = device ms per outer iteration."""
+    from cfdapp_b200 import cfdb
+    rank, world, local = dist_info()
+    if rank != 0:
+        return 0
+    if not cfdb.cuda_available():
+        raise SystemExit("bench.py: no sm_100 device visible (the product has no CPU path)")
+    ctx = cfdb.Context(local)
+    n = a.n3d
+    case = cfdb.SimpleCase.cavity(3, n, lid=1.0, mu=1e-3)
+    sim = cfdb.Simple(ctx, case, cavity3d_settings("learned"))
+    sim.set_state(None, None, None, None)
+    sim.iterate(a.warmup)
+    clocks = ClockSampler(local)
+    clocks.start()
+    launches0 = ctx.launches()
+    r = sim.iterate(a.steps)
+    clk = clocks.stop()
+    launches = ctx.launches() - launches0
+    u, v, w, p, _ = sim.get_state()
+    sim.close()
+    # the same state, one iteration with the Jacobi-PCG p' solve
+    jac = cfdb.Simple(ctx, case, cavity3d_settings("jacobi"))
+    jac.set_state(u, v, w, p)
+    rj = jac.iterate(1)
+    jac.close()
+    line = {
+        "metric": CAVITY3D_METRIC, "value": r.device_ms / max(r.iterations, 1), "unit": "ms",
+        "n_gpus": 1, "steps": r.iterations, "warmup": a.warmup,
+        "ms_per_step": r.device_ms / max(r.iterations, 1), "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64 (SIMPLE, FCG) / f32 (V-cycle)",
+        "data": "synthetic",
+        "config": {"workload": f"{n}^3 lid-driven cavity, Re 1000, linear upwind, Rhie-Chow, "
+                               "BiCGSTAB momentum, learned-FCG p' to 1e-8, from rest after "
+                               f"{a.warmup} outer iterations",
+                   "cells": n ** 3},
+        "pprime_ms_per_iteration": r.pressure_solve_ms / max(r.iterations, 1),
+        "pprime_share": r.pressure_solve_ms / r.device_ms if r.device_ms else None,
+        "pprime_iterations_per_outer": r.pressure_linear_iterations / max(r.iterations, 1),
+        "momentum_ms_per_iteration": r.momentum_solve_ms / max(r.iterations, 1),
+        "jacobi_pcg_outer_iteration_ms": rj.device_ms,
+        "jacobi_pcg_pprime_ms": rj.pressure_solve_ms,
+        "jacobi_pcg_pprime_iterations": rj.pressure_linear_iterations,
+        "status": r.status, "final": r.final,
+        "gpu_launches": launches, "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+    ctx.close()
+    return 0
+
+
 # ------------------------------------------------------------------ device arm
 def main():
     a = parse()
     if a.workload == "batched":
         return run_batched(a)
+    if a.workload == "cavity3d":
+        return run_cavity3d(a)
     grids = grids_from(a)
     if a.impl == "reference":
         return run_reference(a, grids)

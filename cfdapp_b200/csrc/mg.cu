@@ -1235,7 +1235,30 @@ __global__ void k_fcg_update(int64_t n, FcgState* S, double* __restrict__ r,
   double* __restrict__ x = S->x;
   double acc[1] = {0.0};
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n; c += stride) {
+  const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  // four cells per thread in 16-byte vectors, then the remainder one by
+  // one; the solver's own arrays start 256-byte aligned, the caller's x may
+  // not (then every cell takes the scalar loop)
+  const bool vec = (reinterpret_cast<uintptr_t>(x) & 15u) == 0;
+  const int64_t n4 = vec ? n / 4 : 0;
+  for (int64_t g = tid; g < n4; g += stride) {
+    const int64_t c = 4 * g;
+    V4<double> xv = ld4(x + c), rv = ld4(r + c);
+    const V4<double> pv = ld4(p + c), qv = ld4(q + c);
+    V4<float> rf;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      xv.v[u] = fma(alpha, pv.v[u], xv.v[u]);
+      const double rn = fma(-alpha, qv.v[u], rv.v[u]);
+      rv.v[u] = rn;
+      rf.v[u] = (float)rn;
+      acc[0] += rn * rn;
+    }
+    st4(x + c, xv);
+    st4(r + c, rv);
+    st4(r32 + c, rf);
+  }
+  for (int64_t c = 4 * n4 + tid; c < n; c += stride) {
     x[c] = fma(alpha, p[c], x[c]);
     const double rn = fma(-alpha, q[c], r[c]);
     r[c] = rn;
@@ -1421,7 +1444,8 @@ void launch_init(LearnedSolver* s, const FineOperator& op, Loop h, cudaStream_t 
 template <int DIM>
 void launch_dir_q(LearnedSolver* s, const FineOperator& op, Loop h, cudaStream_t st) {
   const Seg sg = make_quad_seg<DIM>(op.A.nx, op.A.ny, op.A.nz);
-  k_fcg_dir_q<DIM><<<quad_grid<DIM>(sg), Quad<DIM>::TX * Quad<DIM>::TY, 0, st>>>(
+  const int grid = quad_grid<DIM>(sg, (int64_t)dir_blocks_per_sm<DIM>() * 148);
+  k_fcg_dir_q<DIM><<<grid, Quad<DIM>::TX * Quad<DIM>::TY, 0, st>>>(
       op.A, sg, s->S, s->z32, s->p0, s->p1, s->q, s->r, s->partials, h);
 }
 

@@ -33,10 +33,10 @@ bool quad_ok(int nx) {
   return nx % 4 == 0 && nx >= quad_px<DIM>();
 }
 
-// Blocks of a quad pass: 2D blocks are 64 threads, so up to 32 per SM.
+// Blocks of a quad pass: 2D blocks are 64 threads, so up to 32 per SM; a
+// pass whose blocks need more registers passes its own cap.
 template <int DIM>
-int quad_grid(const Seg& s) {
-  const int64_t cap = DIM == 2 ? 148 * 32 : kGridCap;
+int quad_grid(const Seg& s, int64_t cap = DIM == 2 ? 148 * 32 : kGridCap) {
   const int64_t per = std::max<int64_t>(1, (s.items + cap - 1) / cap);
   return (int)std::max<int64_t>(1, (s.items + per - 1) / per);
 }
@@ -349,8 +349,15 @@ __global__ void __launch_bounds__(Quad<DIM>::TX* Quad<DIM>::TY)
 }
 
 // The quad counterpart of the FCG direction pass (see k_fcg_dir).
+// Resident blocks per SM of the direction pass (its register budget); its
+// grid is one wave of them, so every block marches a long run of planes.
 template <int DIM>
-__global__ void __launch_bounds__(Quad<DIM>::TX* Quad<DIM>::TY, DIM == 3 ? 2 : 8)
+constexpr int dir_blocks_per_sm() {
+  return DIM == 3 ? 2 : 8;
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(Quad<DIM>::TX* Quad<DIM>::TY, dir_blocks_per_sm<DIM>())
     k_fcg_dir_q(OpView<double> A, Seg sg, FcgState* S, const float* __restrict__ z, double* P0,
                 double* P1, double* __restrict__ q, const double* __restrict__ r, double* partials,
                 Loop h) {
