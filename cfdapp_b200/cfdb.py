@@ -854,3 +854,58 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+# ------------------------------------------------------------ result files
+def _results_sigs(L):
+    vp, i64 = C.c_void_p, C.c_int64
+    dp = C.POINTER(C.c_double)
+    ip = C.POINTER(C.c_int)
+    L.cfdb_write_results.argtypes = [C.POINTER(_SimpleCase), dp, dp, dp, dp, dp, i64, C.c_double,
+                                     C.c_char_p, ip]
+    L.cfdb_simple_write_results.argtypes = [vp, dp, i64, C.c_double, C.c_char_p, ip]
+    L.cfdb_batch_write_results.argtypes = [vp, C.c_int, C.c_char_p, ip]
+
+
+def write_results(case: SimpleCase, u, v, w, p, history, global_imbalance: float, directory: str,
+                  lib=None) -> bool:
+    """fields.csv, residuals.csv and solution.vtk in the reference's formats
+    (host only); history: rows of {u, v, w, p, continuity}.  Returns whether
+    the field files were written (all values finite)."""
+    L = lib or load()
+    _results_sigs(L)
+    n = case.cells()
+    arr = [np.ascontiguousarray(a if a is not None and np.size(a) else np.zeros(n), dtype=np.float64)
+           for a in (u, v, w, p)]
+    h = np.ascontiguousarray(np.asarray(history, dtype=np.float64).reshape(-1, 5))
+    done = C.c_int()
+    st = L.cfdb_write_results(C.byref(case.c()), *[_dp(a) for a in arr], _dp(h.reshape(-1)),
+                              h.shape[0], float(global_imbalance), directory.encode(),
+                              C.byref(done))
+    if st != 0:
+        raise CfdbError(f"cfdb_write_results failed ({st})")
+    return bool(done.value)
+
+
+def _simple_write_results(self, history, global_imbalance: float, directory: str) -> bool:
+    _results_sigs(self.ctx.lib)
+    h = np.ascontiguousarray(np.asarray(history, dtype=np.float64).reshape(-1, 5))
+    done = C.c_int()
+    self.ctx.check(self.ctx.lib.cfdb_simple_write_results(self._h, _dp(h.reshape(-1)), h.shape[0],
+                                                          float(global_imbalance),
+                                                          directory.encode(), C.byref(done)),
+                   "cfdb_simple_write_results")
+    return bool(done.value)
+
+
+def _batch_write_results(self, k: int, directory: str) -> bool:
+    _results_sigs(self.ctx.lib)
+    done = C.c_int()
+    self.ctx.check(self.ctx.lib.cfdb_batch_write_results(self._h, k, directory.encode(),
+                                                         C.byref(done)),
+                   "cfdb_batch_write_results")
+    return bool(done.value)
+
+
+Simple.write_results = _simple_write_results
+Batch.write_results = _batch_write_results

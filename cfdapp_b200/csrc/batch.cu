@@ -178,6 +178,7 @@ struct cfdb_batch {
   int n = 0, dim = 0;
   cfdb_simple_settings st{};
   std::vector<BCase> hc;
+  std::vector<cfdb_simple_case> cases;  // as given (for the result files)
   std::vector<int64_t> cells, faces;
   int64_t cpool = 0, fpool = 0;
   BatchDev D{};
@@ -568,6 +569,7 @@ cfdb_status cfdb_batch_create(cfdb_context* ctx, int ncases, const cfdb_simple_c
   b->face_flux = st->face_flux == CFDB_FLUX_AUTOMATIC ? (dim == 2 ? CFDB_FLUX_LINEAR : CFDB_FLUX_RHIE_CHOW)
                                                       : st->face_flux;
   b->hc.resize(ncases);
+  b->cases.assign(cases, cases + ncases);
   b->cells.resize(ncases);
   b->faces.resize(ncases);
   int64_t cp = 0, fp = 0;
@@ -901,6 +903,29 @@ cfdb_status cfdb_batch_history(cfdb_batch* b, int k, double* history, int64_t ca
                             sizeof(double) * 5 * kept)))
     return rc;
   if (rows) *rows = kept;
+  return CFDB_OK;
+}
+
+cfdb_status cfdb_batch_write_results(cfdb_batch* b, int k, const char* dir, int* fields_written) {
+  if (!b || k < 0 || k >= b->n || !dir) return CFDB_ERR_INVALID_ARGUMENT;
+  const BCase& K = b->hc[k];
+  const size_t n = (size_t)K.G.nc;
+  std::vector<double> u(n), v(n), w(n), p(n);
+  cfdb_status rc = cfdb_batch_get_state(b, k, u.data(), v.data(), w.data(), p.data(), nullptr);
+  if (rc != CFDB_OK) return rc;
+  int64_t outer = 0;
+  std::vector<double> res(BR_COUNT);
+  if ((rc = d2h(b, &outer, b->D.outer + k, sizeof(int64_t))) ||
+      (rc = d2h(b, res.data(), b->D.res + (size_t)k * BR_COUNT, sizeof(double) * BR_COUNT)))
+    return rc;
+  const int64_t rows = std::min(outer, b->history_cap);
+  std::vector<double> hist(5 * (size_t)std::max<int64_t>(rows, 1));
+  if (rows > 0 && (rc = d2h(b, hist.data(), b->D.history + (size_t)k * b->history_cap * 5,
+                            sizeof(double) * 5 * rows)))
+    return rc;
+  rc = cfdb_write_results(&b->cases[k], u.data(), v.data(), w.data(), p.data(), hist.data(), rows,
+                          res[BR_GLOB], dir, fields_written);
+  if (rc != CFDB_OK) return set_error(b->ctx, rc, "cannot write the result files");
   return CFDB_OK;
 }
 

@@ -540,6 +540,20 @@ cfdb_status cfdb_simple_pprime_faces(cfdb_simple* s, double* faces, int* pinned,
   return CFDB_OK;
 }
 
+cfdb_status cfdb_simple_write_results(cfdb_simple* s, const double* history, int64_t rows,
+                                      double global_imbalance, const char* dir,
+                                      int* fields_written) {
+  if (!s || !dir) return CFDB_ERR_INVALID_ARGUMENT;
+  const size_t n = (size_t)s->n;
+  std::vector<double> u(n), v(n), w(n), p(n);
+  cfdb_status rc = cfdb_simple_get_state(s, u.data(), v.data(), w.data(), p.data(), nullptr);
+  if (rc != CFDB_OK) return rc;
+  rc = cfdb_write_results(&s->cs, u.data(), v.data(), w.data(), p.data(), history, rows,
+                          global_imbalance, dir, fields_written);
+  if (rc != CFDB_OK) return set_error(s->ctx, rc, "cannot write the result files");
+  return CFDB_OK;
+}
+
 cfdb_status cfdb_simple_pressure_gradient(cfdb_simple* s, double* gx, double* gy, double* gz) {
   if (!s || !gx || !gy) return CFDB_ERR_INVALID_ARGUMENT;
   gradient(s, s->d_ptype, s->d_pvalue, s->p, s->gradP);

@@ -283,6 +283,26 @@ CFDB_API cfdb_status cfdb_simple_assemble_momentum(cfdb_simple* s, int comp, dou
 CFDB_API cfdb_status cfdb_simple_iterate(cfdb_simple* s, int64_t n, double* history,
                                          cfdb_simple_result* result);
 
+/* Result files of a SIMPLE run in the reference's export formats
+ * (ResultExporter::write, src/io/ResultExporter.cpp:36-110, without its
+ * metadata.json): dir/residuals.csv (CSVWriter::writeResiduals) always, and,
+ * when every u, v, (w,) p value is finite, dir/fields.csv
+ * (CSVWriter::writeFields / writeFields3D) and dir/solution.vtk
+ * (VTKWriter::writeSolution in 2D, writeCellFields in 3D); dir and its
+ * parents are created.  Byte for byte what the reference writes for the same
+ * values.  _results: host fields (u, v, w (3D), p in cell order), history
+ * rows of 5 doubles {u, v, w, p, continuity} as cfdb_simple_solve writes
+ * them, the run's final global mass imbalance; *fields_written (may be NULL)
+ * = 1 when the field files were written.  Host only, no device needed. */
+CFDB_API cfdb_status cfdb_write_results(const cfdb_simple_case* cs, const double* u, const double* v,
+                                        const double* w, const double* p, const double* history,
+                                        int64_t rows, double global_imbalance, const char* dir,
+                                        int* fields_written);
+/* The same files from a session's device fields (downloaded first). */
+CFDB_API cfdb_status cfdb_simple_write_results(cfdb_simple* s, const double* history, int64_t rows,
+                                               double global_imbalance, const char* dir,
+                                               int* fields_written);
+
 /* ---------------------------------------------------------- batched SIMPLE */
 
 /* No counterpart in the reference, which solves one case per process
@@ -361,6 +381,11 @@ CFDB_API cfdb_status cfdb_batch_results(cfdb_batch* b, cfdb_simple_result* resul
 /* Case k's residual history: up to cap rows of 5 doubles; *rows = rows kept. */
 CFDB_API cfdb_status cfdb_batch_history(cfdb_batch* b, int k, double* history, int64_t cap,
                                         int64_t* rows);
+
+/* Case k's result files (see cfdb_write_results) from the batch's device
+ * fields and the history it kept (history_cap rows at most). */
+CFDB_API cfdb_status cfdb_batch_write_results(cfdb_batch* b, int k, const char* dir,
+                                              int* fields_written);
 
 /* Host-only planning of the batch's work lists (no device needed).
  * Tiles: case k's count[k] items split into ceil(count[k]/tile) tiles;

@@ -67,7 +67,7 @@ def test_poisson_matches_golden(name):
 
 
 @pytest.mark.parametrize("name", [n for n in _fixtures("")
-                                  if not n.startswith("poisson")])
+                                  if not n.startswith(("poisson", "results_"))])
 def test_simple_matches_golden(name):
     g = np.load(os.path.join(GOLDEN, name + ".npz"))
     meta = json.loads(str(g["meta"]))
