@@ -70,6 +70,18 @@ def dist_info():
     return rank, world, local
 
 
+def combine_over_ranks(dist, device, ms, work=0.0):
+    """Whole-job figures of a multi-rank run: the max over ranks of the
+    device time and the sum over ranks of the work done (every rank takes the
+    same two collective steps, in the same order)."""
+    import torch
+    t = torch.tensor([float(ms)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    w = torch.tensor([float(work)], device=device, dtype=torch.float64)
+    dist.all_reduce(w, op=dist.ReduceOp.SUM)
+    return float(t.item()), float(w.item())
+
+
 # ------------------------------------------------------------------ clocks
 class ClockSampler:
     """nvidia-smi clock/throttle sampling during the timed region."""
@@ -354,12 +366,7 @@ def run_batched(a):
     work = float(((it1 - it0) * cells).sum())
     dev_ms = st["device_ms"]
     if torch_dist:
-        import torch
-        t = torch.tensor([dev_ms], device=f"cuda:{local}", dtype=torch.float64)
-        torch_dist.all_reduce(t, op=torch_dist.ReduceOp.MAX)
-        w = torch.tensor([work], device=f"cuda:{local}", dtype=torch.float64)
-        torch_dist.all_reduce(w, op=torch_dist.ReduceOp.SUM)
-        dev_ms, work = float(t.item()), float(w.item())
+        dev_ms, work = combine_over_ranks(torch_dist, f"cuda:{local}", dev_ms, work)
     value = work / (dev_ms * 1e-3) if dev_ms > 0 else 0.0
     # e2e through the public API: upload every case's state from host arrays,
     # run the steps, download every case's fields
@@ -585,10 +592,7 @@ def main():
     clk = clocks.stop()
     ms_step = statistics.mean(step_ms)
     if torch_dist:
-        import torch
-        t = torch.tensor([ms_step], device=f"cuda:{local}")
-        torch_dist.all_reduce(t, op=torch_dist.ReduceOp.MAX)
-        ms_step = float(t.item())
+        ms_step, _ = combine_over_ranks(torch_dist, f"cuda:{local}", ms_step)
 
     # ---- e2e through the C ABI with host buffers
     e2e = []
