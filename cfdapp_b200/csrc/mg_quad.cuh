@@ -462,3 +462,115 @@ __global__ void __launch_bounds__(Quad<DIM>::TX* Quad<DIM>::TY, dir_blocks_per_s
     S->alpha = alpha;
   });
 }
+
+// The direction pass without a marching tile: one thread per four-cell quad,
+// its six neighbour values read straight from global memory (L1/L2 serve the
+// re-reads of the neighbouring quads), so a thread keeps little state and
+// many warps stay resident to hide DRAM latency.  Same arithmetic and
+// coefficient order as k_fcg_dir_q.
+template <int DIM>
+__global__ void __launch_bounds__(256) k_fcg_dir_v(OpView<double> A, FcgState* S,
+                                                   const float* __restrict__ z, double* P0,
+                                                   double* P1, double* __restrict__ q,
+                                                   const double* __restrict__ r, double* partials,
+                                                   Loop h) {
+  if (S->done) return;
+  const long long it = S->it;
+  const bool first = (it == 0);
+  const double beta = first ? 0.0 : S->beta;
+  double* __restrict__ pn = (it & 1) ? P1 : P0;
+  const double* __restrict__ po = (it & 1) ? P0 : P1;
+  const int nx = A.nx, ny = A.ny, nz = A.nz, qxn = nx >> 2;
+  const int nq = qxn * ny * nz;
+  const int64_t plane = (int64_t)nx * ny;
+  auto val4 = [&](int64_t c) {
+    const V4<float> zz = ld4(z + c);
+    V4<double> v;
+    if (first) {
+#pragma unroll
+      for (int t = 0; t < 4; ++t) v.v[t] = (double)zz.v[t];
+    } else {
+      const V4<double> p = ld4(po + c);
+#pragma unroll
+      for (int t = 0; t < 4; ++t) v.v[t] = fma(-beta, p.v[t], (double)zz.v[t]);
+    }
+    return v;
+  };
+  auto val1 = [&](int64_t c) { return first ? (double)z[c] : fma(-beta, po[c], (double)z[c]); };
+  const V4<double> zero{{0.0, 0.0, 0.0, 0.0}};
+  double acc[2] = {0.0, 0.0};
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < nq; g += gridDim.x * blockDim.x) {
+    const int qx = g % qxn, rest = g / qxn;
+    const int j = rest % ny, k = rest / ny;
+    const int i0 = 4 * qx;
+    const int64_t c = i0 + (int64_t)nx * (j + (int64_t)ny * k);
+    const V4<double> v = val4(c);
+    const double wl = i0 > 0 ? val1(c - 1) : 0.0;
+    const double er = i0 + 4 < nx ? val1(c + 4) : 0.0;
+    const V4<double> s = (DIM == 3 && j > 0) ? val4(c - nx) : zero;
+    const V4<double> n = (DIM == 3 && j + 1 < ny) ? val4(c + nx) : zero;
+    const V4<double> b = k > 0 ? val4(c - plane) : zero;
+    const V4<double> t = k + 1 < nz ? val4(c + plane) : zero;
+    double fx[5];
+    if (A.fx) {
+      const int64_t bx = i0 + (int64_t)(nx + 1) * (j + (int64_t)ny * k);
+#pragma unroll
+      for (int u = 0; u < 5; ++u) fx[u] = A.fx[bx + u];
+    } else {
+#pragma unroll
+      for (int u = 0; u < 5; ++u) fx[u] = A.tx[i0 + u];
+    }
+    V4<double> yl, yh, zl, zh;
+    if (A.fy) {
+      const int64_t by = i0 + (int64_t)nx * (j + (int64_t)(ny + 1) * k);
+      yl = ld4(A.fy + by);
+      yh = ld4(A.fy + by + nx);
+    } else {
+      const double a = A.ty[j], bb = A.ty[j + 1];
+      yl = V4<double>{{a, a, a, a}};
+      yh = V4<double>{{bb, bb, bb, bb}};
+    }
+    if (A.fz) {
+      zl = ld4(A.fz + c);
+      zh = ld4(A.fz + c + plane);
+    } else {
+      const double a = A.tz[k], bb = A.tz[k + 1];
+      zl = V4<double>{{a, a, a, a}};
+      zh = V4<double>{{bb, bb, bb, bb}};
+    }
+    V4<double> aq;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const double w = u == 0 ? wl : v.v[u - 1];
+      const double e = u == 3 ? er : v.v[u + 1];
+      // diagonal summed in the reference's face order (as load_coef)
+      const double d = ((((fx[u] + fx[u + 1]) + yl.v[u]) + yh.v[u]) + zl.v[u]) + zh.v[u];
+      double off = fx[u] * w;
+      off = fma(fx[u + 1], e, off);
+      off = fma(yl.v[u], s.v[u], off);
+      off = fma(yh.v[u], n.v[u], off);
+      off = fma(zl.v[u], b.v[u], off);
+      off = fma(zh.v[u], t.v[u], off);
+      aq.v[u] = (A.pinned && c + u == A.ref) ? v.v[u] : fma(d, v.v[u], -off);
+    }
+    st4(pn + c, v);
+    st4(q + c, aq);
+    const V4<double> rr = ld4(r + c);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      acc[0] += v.v[u] * aq.v[u];
+      acc[1] += v.v[u] * rr.v[u];
+    }
+  }
+  reduce_last<2>(acc, partials, &S->ticket, [&](const double* tot) {
+    const double pq = tot[0], pr = tot[1];
+    const double alpha = pr / pq;
+    if (!isfinite(pq) || !(pq > 0.0) || !isfinite(alpha)) {
+      stop_loop(S, h, kLearnedStagnated);
+      return;
+    }
+    S->pq = pq;
+    S->pr = pr;
+    S->alpha = alpha;
+  });
+}
