@@ -77,10 +77,11 @@ struct KArgs {
 // with MOMENTUM_FAILURE, a p' solve with PRESSURE_FAILURE; a case whose
 // fields went non-finite earlier in the iteration stops at the p' stage with
 // NONFINITE_STATE.
-// Four resident blocks per SM (64 registers, some spilled to L1): the team
+// Five resident blocks per SM (48 registers, some spilled to L1): the team
 // solves are latency-bound; measured on the 64-case batch, an outer iteration
-// takes 297 ms with two blocks per SM, 222 ms with three and 197 ms with four.
-__global__ void __launch_bounds__(krylov::kThreads, 4) k_batch_krylov(KArgs A) {
+// takes 297 ms with two blocks per SM, 222 ms with three, 197 ms with four
+// and 187 ms with five.
+__global__ void __launch_bounds__(krylov::kThreads, 5) k_batch_krylov(KArgs A) {
   const int k = A.block_case[blockIdx.x];
   if (k < 0) return;
   const BatchDev& B = A.B;

@@ -28,6 +28,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <string>
 
 #include "cfdb_internal.cuh"
@@ -1003,6 +1004,51 @@ struct LevelOps {
   }
 };
 
+// Blocks of `fn` resident on the whole GPU at `threads` threads per block
+// (registers and shared memory permitting), cached per kernel.  A quad pass
+// launched with at most this many blocks runs in one wave.
+int one_wave(const void* fn, int threads) {
+  static std::map<const void*, int> cache;
+  static int sms = 0;
+  auto it = cache.find(fn);
+  if (it != cache.end()) return it->second;
+  if (sms == 0) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1)
+      sms = 148;
+    cudaGetLastError();
+  }
+  int per = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, threads, 0) != cudaSuccess || per < 1) {
+    cudaGetLastError();
+    per = 1;
+  }
+  return cache[fn] = per * sms;
+}
+
+template <int DIM>
+int quad_wave(const void* fn, const Seg& sg) {
+  return quad_grid<DIM>(sg, one_wave(fn, Quad<DIM>::TX * Quad<DIM>::TY));
+}
+
+// Answers every quad pass's occupancy query once, before any stream capture.
+void warm_quad_waves() {
+  const Seg sg{1, 1, 1};
+  quad_wave<2>((const void*)k_res_q<2, false, true>, sg);
+  quad_wave<2>((const void*)k_res_q<2, true, false>, sg);
+  quad_wave<2>((const void*)k_res_q<2, false, false>, sg);
+  quad_wave<2>((const void*)k_sm_q<2, SM_FIRST, false>, sg);
+  quad_wave<2>((const void*)k_sm_q<2, SM_ADD, true>, sg);
+  quad_wave<2>((const void*)k_sm_q<2, SM_ADD, false>, sg);
+  quad_wave<3>((const void*)k_res_q<3, false, true>, sg);
+  quad_wave<3>((const void*)k_res_q<3, true, false>, sg);
+  quad_wave<3>((const void*)k_res_q<3, false, false>, sg);
+  quad_wave<3>((const void*)k_sm_q<3, SM_FIRST, false>, sg);
+  quad_wave<3>((const void*)k_sm_q<3, SM_ADD, true>, sg);
+  quad_wave<3>((const void*)k_sm_q<3, SM_ADD, false>, sg);
+}
+
 template <int DIM>
 void level_res(const MgLevel& M, const LV& LC, const float* x, const float* ec, float cw,
                const float* r, float* res, float* rc, int64_t skip, cudaStream_t st) {
@@ -1018,12 +1064,17 @@ void level_res(const MgLevel& M, const LV& LC, const float* x, const float* ec, 
     }
   } else if (quad_ok<DIM>(M.n[0])) {
     const Seg sg = make_quad_seg<DIM>(M.n[0], M.n[1], M.n[2]);
-    const int g = quad_grid<DIM>(sg);
     constexpr int T = Quad<DIM>::TX * Quad<DIM>::TY;
     const LV L = lv(M);
-    if (rc) k_res_q<DIM, false, true><<<g, T, 0, st>>>(L, LC, sg, x, ec, cw, r, res, rc, skip);
-    else if (ec) k_res_q<DIM, true, false><<<g, T, 0, st>>>(L, LC, sg, x, ec, cw, r, res, rc, skip);
-    else k_res_q<DIM, false, false><<<g, T, 0, st>>>(L, LC, sg, x, ec, cw, r, res, rc, skip);
+    if (rc)
+      k_res_q<DIM, false, true><<<quad_wave<DIM>((const void*)k_res_q<DIM, false, true>, sg), T, 0, st>>>(
+          L, LC, sg, x, ec, cw, r, res, rc, skip);
+    else if (ec)
+      k_res_q<DIM, true, false><<<quad_wave<DIM>((const void*)k_res_q<DIM, true, false>, sg), T, 0, st>>>(
+          L, LC, sg, x, ec, cw, r, res, rc, skip);
+    else
+      k_res_q<DIM, false, false><<<quad_wave<DIM>((const void*)k_res_q<DIM, false, false>, sg), T, 0, st>>>(
+          L, LC, sg, x, ec, cw, r, res, rc, skip);
   } else {
     LevelOps<DIM, 1>::res(M, LC, x, ec, cw, r, res, rc, skip, st);
   }
@@ -1041,15 +1092,17 @@ void level_sm(const MgLevel& M, const LV& LC, const Kern& K, bool first, const f
       k_sm_f<DIM, SM_ADD><<<flat_blocks(M.cells), 256, 0, st>>>(L, LC, K, src, ec, cw, x, skip, pin, r);
   } else if (quad_ok<DIM>(M.n[0])) {
     const Seg sg = make_quad_seg<DIM>(M.n[0], M.n[1], M.n[2]);
-    const int g = quad_grid<DIM>(sg);
     constexpr int T = Quad<DIM>::TX * Quad<DIM>::TY;
     const LV L = lv(M);
     if (first)
-      k_sm_q<DIM, SM_FIRST, false><<<g, T, 0, st>>>(L, LC, sg, K, src, ec, cw, x, skip, pin, r, Hook{});
+      k_sm_q<DIM, SM_FIRST, false><<<quad_wave<DIM>((const void*)k_sm_q<DIM, SM_FIRST, false>, sg), T, 0,
+                                     st>>>(L, LC, sg, K, src, ec, cw, x, skip, pin, r, Hook{});
     else if (hook)
-      k_sm_q<DIM, SM_ADD, true><<<g, T, 0, st>>>(L, LC, sg, K, src, ec, cw, x, skip, pin, r, *hook);
+      k_sm_q<DIM, SM_ADD, true><<<quad_wave<DIM>((const void*)k_sm_q<DIM, SM_ADD, true>, sg), T, 0, st>>>(
+          L, LC, sg, K, src, ec, cw, x, skip, pin, r, *hook);
     else
-      k_sm_q<DIM, SM_ADD, false><<<g, T, 0, st>>>(L, LC, sg, K, src, ec, cw, x, skip, pin, r, Hook{});
+      k_sm_q<DIM, SM_ADD, false><<<quad_wave<DIM>((const void*)k_sm_q<DIM, SM_ADD, false>, sg), T, 0, st>>>(
+          L, LC, sg, K, src, ec, cw, x, skip, pin, r, Hook{});
   } else {
     LevelOps<DIM, 1>::sm(M, LC, K, first, src, ec, cw, x, skip, pin, r, hook, st);
   }
@@ -1408,7 +1461,10 @@ struct LearnedSolver {
   }
 };
 
-LearnedSolver* learned_create() { return new LearnedSolver(); }
+LearnedSolver* learned_create() {
+  warm_quad_waves();
+  return new LearnedSolver();
+}
 
 void learned_destroy(LearnedSolver* s) {
   if (!s) return;

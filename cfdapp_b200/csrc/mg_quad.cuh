@@ -146,8 +146,10 @@ __device__ __forceinline__ void coef4(const LV& L, int i0, int j, int k, float (
 }
 
 // The quad counterpart of k_res (see there).
+// 3D: four resident blocks per SM (64 registers, no spills): 2.6 % faster
+// per FCG iteration at 256^3; 2D keeps the compiler's own allocation.
 template <int DIM, bool PRO, bool RESTRICT>
-__global__ void __launch_bounds__(Quad<DIM>::TX* Quad<DIM>::TY)
+__global__ void __launch_bounds__(Quad<DIM>::TX* Quad<DIM>::TY, DIM == 3 ? 4 : 0)
     k_res_q(LV L, LV C, Seg sg, const float* __restrict__ x, const float* __restrict__ ec, float cw,
             const float* __restrict__ r, float* __restrict__ res, float* __restrict__ rc,
             int64_t skip) {

@@ -42,9 +42,9 @@ struct GridTeam {
   __device__ bool sync() const { return grid_sync(s); }
 };
 
-// Three resident blocks per SM (80 registers): the momentum solves of the
-// 256^3 cavity run 12 % faster per outer iteration than with two.
-__global__ void __launch_bounds__(kThreads, 3) stencil_krylov(SParams P, GridSync sync) {
+// Four resident blocks per SM (64 registers): the 256^3 cavity's outer
+// iteration takes 111 ms with two, 97 ms with three and 92 ms with four.
+__global__ void __launch_bounds__(kThreads, 4) stencil_krylov(SParams P, GridSync sync) {
   const GridTeam T{sync};
   krylov::krylov_run(P, T);
 }
