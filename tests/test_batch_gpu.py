@@ -183,3 +183,33 @@ def test_profiled_iteration_times_every_launch(ctx):
     assert ids.count(-1) == 2 and ids.count(-2) == 1 and all(ms >= 0 for _, ms in prof)
     assert all(r["iterations"] == 1 for r in b.results())
     b.close()
+
+
+def test_batch_edge_cases(ctx):
+    """One-case and minimal-grid batches, mixed families in one batch, and the
+    configurations a batch refuses."""
+    from cfdapp_b200.cfdb import (Batch, CfdbError, LinearSolverSettings, SIMPLESettings,
+                                  SimpleCase)
+    s = SIMPLESettings(max_iterations=8)
+    cases = [SimpleCase.cavity(2, 2), SimpleCase.channel(9, 3, 3.0, 1.0),
+             SimpleCase.cavity(2, 33)]
+    b = Batch(ctx, cases, s)
+    for k in range(len(cases)):
+        b.set_state(k)
+    b.iterate(20)
+    res = b.results()
+    for k, case in enumerate(cases):
+        _check_against_single(ctx, case, s, b.get_state(k), res[k], bar=1e-7)
+    b.close()
+    one = Batch(ctx, [SimpleCase.cavity(2, 17)], s)
+    one.set_state(0)
+    one.iterate(8)
+    _check_against_single(ctx, SimpleCase.cavity(2, 17), s, one.get_state(0), one.results()[0],
+                          bar=1e-7)
+    one.close()
+    with pytest.raises(CfdbError):
+        Batch(ctx, [SimpleCase.cavity(2, 8), SimpleCase.cavity(3, 6)], s)
+    learned = SIMPLESettings(max_iterations=8, pressure_solver=LinearSolverSettings(
+        type="cg", preconditioner="learned_mg"))
+    with pytest.raises(CfdbError):
+        Batch(ctx, [SimpleCase.cavity(2, 8)], learned)
