@@ -356,6 +356,23 @@ class POperator:
                                                               C.byref(res)), "cfdb_poperator_solve_host")
         return self._result(res, hist, cap, x)
 
+    def solve_inplace(self, b: np.ndarray, x: np.ndarray, settings: LinearSolverSettings,
+                      history_cap: int = 0) -> SolverResult:
+        """Host buffers used in place (float64, contiguous; pinned buffers let
+        the copies run at full link speed): b in, x0 in x, solution out in x."""
+        for a in (b, x):
+            if a.dtype != np.float64 or not a.flags["C_CONTIGUOUS"] or a.size != self.cells:
+                raise CfdbError("solve_inplace needs contiguous float64 arrays of the grid's size")
+        hist = np.zeros(max(history_cap, 1))
+        res = _LinResult()
+        cs = settings.c()
+        self._precision = cs.precision
+        self._precond = cs.preconditioner
+        self.ctx.check(self.ctx.lib.cfdb_poperator_solve_host(self.ctx.handle, self._h, C.byref(cs),
+                                                              _dp(b), _dp(x), _dp(hist), history_cap,
+                                                              C.byref(res)), "cfdb_poperator_solve_host")
+        return self._result(res, hist, history_cap, x)
+
     def solve_device(self, b_dev: int, x_dev: int, settings: LinearSolverSettings,
                      history_cap: int = 0) -> SolverResult:
         """Device-resident b and x (x holds x0 on entry)."""
