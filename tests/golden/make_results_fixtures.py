@@ -1,11 +1,13 @@
 """Fixtures of the reference's result-file formats, taken from two of the
-reference's committed example runs (cases/lid_driven_cavity, 20x20, and
-cases/lid_driven_cavity_3d, 16^3): the field values and residual history
+reference's committed example runs (cases/lid_driven_cavity, 20x20,
+cases/lid_driven_cavity_3d, 16^3, and cases/poiseuille_flow, 64x8): the field values and residual history
 parsed back from their fields.csv / residuals.csv (17 significant digits
 round-trip exactly), the final global mass imbalance, the grid, and the
 SHA-256 and size of each committed fields.csv, residuals.csv and
 solution.vtk.  tests/test_results_io.py writes the same values through
-cfdb_write_results and compares the files byte for byte by hash.
+cfdb_write_results and compares the files byte for byte by hash.  The case
+input files (case.json and the five files it names) are copied to
+tests/golden/cases/<case>/ for tests/test_cases.py.
 
     python tests/golden/make_results_fixtures.py <reference checkout>
 """
@@ -18,7 +20,10 @@ import sys
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-CASES = {"results_cavity2d_20": "lid_driven_cavity", "results_cavity3d_16": "lid_driven_cavity_3d"}
+CASES = {"results_cavity2d_20": "lid_driven_cavity", "results_cavity3d_16": "lid_driven_cavity_3d",
+         "results_channel2d_64x8": "poiseuille_flow"}
+CASE_FILES = ("case.json", "geometry.json", "mesh.json", "physics.json", "boundaries.json",
+              "solver.json")
 
 
 def main(ref):
@@ -55,6 +60,11 @@ def main(ref):
                 "files": files}
         np.savez_compressed(os.path.join(HERE, name + ".npz"), u=u, v=v, w=w, p=p, hist=hist,
                             meta=json.dumps(meta))
+        dst = os.path.join(HERE, "cases", case)
+        os.makedirs(dst, exist_ok=True)
+        for fn in CASE_FILES:
+            with open(os.path.join(base, fn), "rb") as fi, open(os.path.join(dst, fn), "wb") as fo:
+                fo.write(fi.read())
         print(name, meta["n"], R.shape[0], "rows")
 
 

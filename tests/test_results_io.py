@@ -1,7 +1,7 @@
 """The result-file writer (cfdb_write_results) against the reference's own
 committed example outputs, byte for byte: the field values and residual
-history of cases/lid_driven_cavity (20x20) and cases/lid_driven_cavity_3d
-(16^3), parsed back from the reference's files (tests/golden/
+history of cases/lid_driven_cavity (20x20), cases/lid_driven_cavity_3d
+(16^3) and cases/poiseuille_flow (64x8), parsed back from the reference's files (tests/golden/
 make_results_fixtures.py), written again must hash to the reference's
 fields.csv, residuals.csv and solution.vtk.  No device needed."""
 import hashlib
@@ -26,7 +26,8 @@ def _case(meta):
     return cfdb.SimpleCase(dim, tuple(meta["n"]), tuple(meta["length"]) + (1.0,) * (3 - dim))
 
 
-@pytest.mark.parametrize("name", ["results_cavity2d_20", "results_cavity3d_16"])
+@pytest.mark.parametrize("name", ["results_cavity2d_20", "results_cavity3d_16",
+                                  "results_channel2d_64x8"])
 def test_writer_reproduces_the_reference_files(tmp_path, name):
     g, meta = _fixture(name)
     d = str(tmp_path / "results")
