@@ -443,6 +443,18 @@ CFDB_API cfdb_status cfdb_mg_loss_grad(cfdb_context* ctx, cfdb_poperator* op, in
                                        const float* e_host, double* loss, double* grad_kernels,
                                        double* grad_coarse);
 
+/* ------------------------------------------------------------------ self-test */
+
+/* No counterpart in the reference.  Exercises the bounded device-side wait
+ * that the persistent kernels' grid and team barriers use: a two-block kernel
+ * waits on a barrier sized for three blocks, which can never complete; after
+ * timeout_s (0 < timeout_s <= 10) the blocks give up, raise the barrier's
+ * error flag and return.  Returns CFDB_ERR_DEVICE_TIMEOUT (the expected
+ * outcome) with *blocks_released = the number of blocks whose barrier call
+ * reported the failure (2); the context stays usable.  No GPU fault. */
+CFDB_API cfdb_status cfdb_selftest_wait_timeout(cfdb_context* ctx, double timeout_s,
+                                                int* blocks_released);
+
 /* ------------------------------------------------------ allocation-free solve */
 
 /* No counterpart in the reference.  The FP64 Jacobi-PCG of the uniform p'
