@@ -29,6 +29,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
 
 #include "cfdb_internal.cuh"
@@ -1008,8 +1009,10 @@ struct LevelOps {
 // (registers and shared memory permitting), cached per kernel.  A quad pass
 // launched with at most this many blocks runs in one wave.
 int one_wave(const void* fn, int threads) {
+  static std::mutex mu;  // contexts on other host threads share the cache
   static std::map<const void*, int> cache;
   static int sms = 0;
+  std::lock_guard<std::mutex> lock(mu);
   auto it = cache.find(fn);
   if (it != cache.end()) return it->second;
   if (sms == 0) {
