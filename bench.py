@@ -247,6 +247,15 @@ def _estimate_iterations(O, dim, n):
     return int(r.iterations * n / m)
 
 
+def _traffic(key):
+    """DRAM bytes per launch recorded from an ncu capture (profiles/traffic.json)."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            return json.load(f).get(key)
+    except (OSError, ValueError):
+        return None
+
+
 # ------------------------------------------------------------------ batched SIMPLE
 BATCH_SIDES = (64, 96, 128, 192, 256, 384, 512)
 BATCH_METRIC = "batched SIMPLE cell outer-iterations per second"
@@ -412,7 +421,8 @@ def run_batched(a):
             "roofline": {"bound": "hbm", "kernel": "batched p' Jacobi-CG team kernel",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak if achieved else None,
-                         "peak_source": f"{peak_kind} hbm_gbs", "traffic": None},
+                         "peak_source": f"{peak_kind} hbm_gbs",
+                         "traffic": _traffic("batched_pprime_dram_bytes_per_launch")},
             "e2e": {"value": e2e_work / (e2e_ms * 1e-3), "unit": "cell outer-iterations/s",
                     "h2d_bytes_per_step": h2d // max(a.steps, 1),
                     "d2h_bytes_per_step": d2h // max(a.steps, 1)},

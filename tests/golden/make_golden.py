@@ -3,7 +3,7 @@ own CPU code (oracle/_ref/ref_driver, built from the reference sources by
 oracle/Makefile.ref).  Run from the repository root:
 
     make -f oracle/Makefile.ref REF=<reference checkout> -j8
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [fixture names]
 
 Each fixture is a compressed .npz of the reference's outputs plus its JSON
 summary; the oracle is checked against them in tests/test_oracle_pin.py.
@@ -27,6 +27,8 @@ SIMPLE = {
     # the reference's committed 20x20 cavity case (BiCGSTAB p' solve)
     "cavity2d_20_bicgstab": ("dim=2 nx=20 ny=20 psolver=bicgstab ppre=none pabs=1e-10 prel=1e-8 "
                              "pmax=2000 outer=6000", ["u", "v", "p", "flux"]),
+    # configuration 1 itself: the 129x129 Re-100 cavity, Jacobi-CG p', to convergence
+    "cavity2d_129_config1": ("dim=2 nx=129 ny=129 outer=20000", ["u", "v", "p", "flux"]),
     # config-1 settings (Jacobi-CG p') on a small grid, to convergence
     "cavity2d_16_jacobicg": ("dim=2 nx=16 ny=16 outer=6000", ["u", "v", "p", "flux"]),
     "cavity2d_16_lud": ("dim=2 nx=16 ny=16 scheme=lud outer=200", ["u", "v", "p", "flux"]),
@@ -45,8 +47,10 @@ def run(cmd, args, out):
     return json.loads(r.stdout)
 
 
-def main():
+def main(only=()):
     for name, args in POISSON.items():
+        if only and name not in only:
+            continue
         with tempfile.TemporaryDirectory() as d:
             meta = run("poisson", args, d)
             np.savez_compressed(os.path.join(HERE, name + ".npz"),
@@ -56,6 +60,8 @@ def main():
                                 meta=json.dumps({**meta, "args": args}))
             print(name, meta["status"], meta["iterations"])
     for name, (args, fields) in SIMPLE.items():
+        if only and name not in only:
+            continue
         with tempfile.TemporaryDirectory() as d:
             meta = run("simple", args, d)
             arrays = {f: np.fromfile(os.path.join(d, f + ".bin")) for f in fields}
@@ -66,4 +72,5 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    import sys
+    main(tuple(sys.argv[1:]))  # fixture names to (re)generate; all when none
