@@ -31,6 +31,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <utility>
 
 #include "cfdb_internal.cuh"
 #include "grid_sync.cuh"
@@ -89,6 +90,17 @@ constexpr int64_t kCoarseCells = 4096;
 constexpr int kMaxCoarse = 8;
 constexpr int kCoarseThreads = 1024;
 constexpr size_t kCoarseSmemCap = 200 * 1024;
+
+// Kernels of the solve body are launched with programmatic dependent launch
+// allowed: each one waits (griddepcontrol.wait) for its predecessor's
+// results before it reads anything, so the launch of a kernel is prepared
+// while its predecessor finishes.  (Letting successors start at the top of
+// each kernel, launch_dependents, was measured 1-3 % slower: their waiting
+// blocks hold resources.)  The wait is a no-op for a kernel launched
+// without the attribute.
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+}
 
 // Thread layout of the tiled kernels: TX x TY threads, each owning CX cells
 // of a plane row strided by TX (so every load instruction is coalesced).
@@ -438,6 +450,7 @@ __global__ void __launch_bounds__(kT) k_res(LV L, LV C, Seg sg, const float* __r
                                             const float* __restrict__ ec, float cw,
                                             const float* __restrict__ r, float* __restrict__ res,
                                             float* __restrict__ rc, int64_t skip) {
+  pdl_enter();
   constexpr int TX = Tile<DIM>::TX, TY = Tile<DIM>::TY, PX = TX * CX;
   __shared__ float buf[2][Rows<TY>::N][PX + 2];
   __shared__ float rows[TY][CX][TX / 2];
@@ -493,6 +506,26 @@ __global__ void __launch_bounds__(kT) k_res(LV L, LV C, Seg sg, const float* __r
 
 enum { SM_FIRST = 0, SM_ADD = 1 };
 
+#ifndef CFDB_PDL
+#define CFDB_PDL 1
+#endif
+
+template <typename... KArgs, typename... Args>
+void launch(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+            Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = CFDB_PDL;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
 // x <- [x] (+ cw P ec) + D^-1/2 (W * (D^-1/2 u)), u = res (SM_ADD) or r with
 // r[skip] = 0 and x = 0 before (SM_FIRST).  pin >= 0: z[pin] = r[pin] (the
 // last sweep of level 0); HOOK: also accumulate z.q for the FCG coefficient.
@@ -501,6 +534,7 @@ __global__ void __launch_bounds__(kT) k_sm(LV L, LV C, Seg sg, Kern K, const flo
                                            const float* __restrict__ ec, float cw,
                                            float* __restrict__ x, int64_t skip, int64_t pin,
                                            const float* __restrict__ r, Hook hk) {
+  pdl_enter();
   constexpr int TX = Tile<DIM>::TX, TY = Tile<DIM>::TY, PX = TX * CX;
   __shared__ float ring[3][Rows<TY>::N][PX + 2];
   double acc[1] = {0.0};
@@ -602,6 +636,7 @@ __device__ __forceinline__ float conv_s(const LV& M, const Kern& K, int i, int j
 // cells (a named barrier instead of the whole block).
 template <int DIM>
 __global__ void __launch_bounds__(kCoarseThreads) k_coarse(CoarsePlan P) {
+  pdl_enter();
   extern __shared__ float4 smem4[];
   float* sm = reinterpret_cast<float*>(smem4);
   const int tid = threadIdx.x, nt = blockDim.x;
@@ -881,6 +916,7 @@ __global__ void __launch_bounds__(256) k_res_f(LV L, LV C, const float* __restri
                                                const float* __restrict__ ec, float cw,
                                                const float* __restrict__ r, float* __restrict__ res,
                                                int64_t skip) {
+  pdl_enter();
   const int64_t n = (int64_t)L.nx * L.ny * L.nz;
   for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
        c += (int64_t)gridDim.x * blockDim.x) {
@@ -908,6 +944,7 @@ template <int DIM>
 __global__ void __launch_bounds__(256) k_restrict_f(LV L, LV C, const float* __restrict__ x,
                                                     const float* __restrict__ r,
                                                     float* __restrict__ rc, int64_t skip) {
+  pdl_enter();
   const int64_t n = (int64_t)C.nx * C.ny * C.nz;
   for (int64_t qc = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; qc < n;
        qc += (int64_t)gridDim.x * blockDim.x) {
@@ -938,6 +975,7 @@ __global__ void __launch_bounds__(256) k_sm_f(LV L, LV C, Kern K, const float* _
                                               const float* __restrict__ ec, float cw,
                                               float* __restrict__ x, int64_t skip, int64_t pin,
                                               const float* __restrict__ r) {
+  pdl_enter();
   const int64_t n = (int64_t)L.nx * L.ny * L.nz;
   for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
        c += (int64_t)gridDim.x * blockDim.x) {
@@ -984,11 +1022,11 @@ struct LevelOps {
     const Seg sg = make_seg<DIM, CX>(M.n[0], M.n[1], M.n[2]);
     const LV L = lv(M);
     if (rc)
-      k_res<DIM, CX, false, true><<<seg_grid(sg), kT, 0, st>>>(L, LC, sg, x, ec, cw, r, res, rc, skip);
+      launch(k_res<DIM, CX, false, true>, seg_grid(sg), kT, 0, st, L, LC, sg, x, ec, cw, r, res, rc, skip);
     else if (ec)
-      k_res<DIM, CX, true, false><<<seg_grid(sg), kT, 0, st>>>(L, LC, sg, x, ec, cw, r, res, rc, skip);
+      launch(k_res<DIM, CX, true, false>, seg_grid(sg), kT, 0, st, L, LC, sg, x, ec, cw, r, res, rc, skip);
     else
-      k_res<DIM, CX, false, false><<<seg_grid(sg), kT, 0, st>>>(L, LC, sg, x, ec, cw, r, res, rc, skip);
+      launch(k_res<DIM, CX, false, false>, seg_grid(sg), kT, 0, st, L, LC, sg, x, ec, cw, r, res, rc, skip);
   }
   static void sm(const MgLevel& M, const LV& LC, const Kern& K, bool first, const float* src,
                  const float* ec, float cw, float* x, int64_t skip, int64_t pin, const float* r,
@@ -997,11 +1035,11 @@ struct LevelOps {
     const LV L = lv(M);
     const int g = seg_grid(sg);
     if (first)
-      k_sm<DIM, CX, SM_FIRST, false><<<g, kT, 0, st>>>(L, LC, sg, K, src, ec, cw, x, skip, pin, r, Hook{});
+      launch(k_sm<DIM, CX, SM_FIRST, false>, g, kT, 0, st, L, LC, sg, K, src, ec, cw, x, skip, pin, r, Hook{});
     else if (hook)
-      k_sm<DIM, CX, SM_ADD, true><<<g, kT, 0, st>>>(L, LC, sg, K, src, ec, cw, x, skip, pin, r, *hook);
+      launch(k_sm<DIM, CX, SM_ADD, true>, g, kT, 0, st, L, LC, sg, K, src, ec, cw, x, skip, pin, r, *hook);
     else
-      k_sm<DIM, CX, SM_ADD, false><<<g, kT, 0, st>>>(L, LC, sg, K, src, ec, cw, x, skip, pin, r, Hook{});
+      launch(k_sm<DIM, CX, SM_ADD, false>, g, kT, 0, st, L, LC, sg, K, src, ec, cw, x, skip, pin, r, Hook{});
   }
 };
 
@@ -1059,25 +1097,25 @@ void level_res(const MgLevel& M, const LV& LC, const float* x, const float* ec, 
     const LV L = lv(M);
     if (rc) {
       const int64_t nc = (int64_t)LC.nx * LC.ny * LC.nz;
-      k_restrict_f<DIM><<<flat_blocks(nc), 256, 0, st>>>(L, LC, x, r, rc, skip);
+      launch(k_restrict_f<DIM>, flat_blocks(nc), 256, 0, st, L, LC, x, r, rc, skip);
     } else if (ec) {
-      k_res_f<DIM, true><<<flat_blocks(M.cells), 256, 0, st>>>(L, LC, x, ec, cw, r, res, skip);
+      launch(k_res_f<DIM, true>, flat_blocks(M.cells), 256, 0, st, L, LC, x, ec, cw, r, res, skip);
     } else {
-      k_res_f<DIM, false><<<flat_blocks(M.cells), 256, 0, st>>>(L, LC, x, ec, cw, r, res, skip);
+      launch(k_res_f<DIM, false>, flat_blocks(M.cells), 256, 0, st, L, LC, x, ec, cw, r, res, skip);
     }
   } else if (quad_ok<DIM>(M.n[0])) {
     const Seg sg = make_quad_seg<DIM>(M.n[0], M.n[1], M.n[2]);
     constexpr int T = Quad<DIM>::TX * Quad<DIM>::TY;
     const LV L = lv(M);
     if (rc)
-      k_res_q<DIM, false, true><<<quad_wave<DIM>((const void*)k_res_q<DIM, false, true>, sg), T, 0, st>>>(
-          L, LC, sg, x, ec, cw, r, res, rc, skip);
+      launch(k_res_q<DIM, false, true>, quad_wave<DIM>((const void*)k_res_q<DIM, false, true>, sg), T,
+             0, st, L, LC, sg, x, ec, cw, r, res, rc, skip);
     else if (ec)
-      k_res_q<DIM, true, false><<<quad_wave<DIM>((const void*)k_res_q<DIM, true, false>, sg), T, 0, st>>>(
-          L, LC, sg, x, ec, cw, r, res, rc, skip);
+      launch(k_res_q<DIM, true, false>, quad_wave<DIM>((const void*)k_res_q<DIM, true, false>, sg), T,
+             0, st, L, LC, sg, x, ec, cw, r, res, rc, skip);
     else
-      k_res_q<DIM, false, false><<<quad_wave<DIM>((const void*)k_res_q<DIM, false, false>, sg), T, 0, st>>>(
-          L, LC, sg, x, ec, cw, r, res, rc, skip);
+      launch(k_res_q<DIM, false, false>, quad_wave<DIM>((const void*)k_res_q<DIM, false, false>, sg), T,
+             0, st, L, LC, sg, x, ec, cw, r, res, rc, skip);
   } else {
     LevelOps<DIM, 1>::res(M, LC, x, ec, cw, r, res, rc, skip, st);
   }
@@ -1090,22 +1128,22 @@ void level_sm(const MgLevel& M, const LV& LC, const Kern& K, bool first, const f
   if (M.cells <= kFlatCells && !hook) {
     const LV L = lv(M);
     if (first)
-      k_sm_f<DIM, SM_FIRST><<<flat_blocks(M.cells), 256, 0, st>>>(L, LC, K, src, ec, cw, x, skip, pin, r);
+      launch(k_sm_f<DIM, SM_FIRST>, flat_blocks(M.cells), 256, 0, st, L, LC, K, src, ec, cw, x, skip, pin, r);
     else
-      k_sm_f<DIM, SM_ADD><<<flat_blocks(M.cells), 256, 0, st>>>(L, LC, K, src, ec, cw, x, skip, pin, r);
+      launch(k_sm_f<DIM, SM_ADD>, flat_blocks(M.cells), 256, 0, st, L, LC, K, src, ec, cw, x, skip, pin, r);
   } else if (quad_ok<DIM>(M.n[0])) {
     const Seg sg = make_quad_seg<DIM>(M.n[0], M.n[1], M.n[2]);
     constexpr int T = Quad<DIM>::TX * Quad<DIM>::TY;
     const LV L = lv(M);
     if (first)
-      k_sm_q<DIM, SM_FIRST, false><<<quad_wave<DIM>((const void*)k_sm_q<DIM, SM_FIRST, false>, sg), T, 0,
-                                     st>>>(L, LC, sg, K, src, ec, cw, x, skip, pin, r, Hook{});
+      launch(k_sm_q<DIM, SM_FIRST, false>, quad_wave<DIM>((const void*)k_sm_q<DIM, SM_FIRST, false>, sg),
+             T, 0, st, L, LC, sg, K, src, ec, cw, x, skip, pin, r, Hook{});
     else if (hook)
-      k_sm_q<DIM, SM_ADD, true><<<quad_wave<DIM>((const void*)k_sm_q<DIM, SM_ADD, true>, sg), T, 0, st>>>(
-          L, LC, sg, K, src, ec, cw, x, skip, pin, r, *hook);
+      launch(k_sm_q<DIM, SM_ADD, true>, quad_wave<DIM>((const void*)k_sm_q<DIM, SM_ADD, true>, sg), T, 0,
+             st, L, LC, sg, K, src, ec, cw, x, skip, pin, r, *hook);
     else
-      k_sm_q<DIM, SM_ADD, false><<<quad_wave<DIM>((const void*)k_sm_q<DIM, SM_ADD, false>, sg), T, 0, st>>>(
-          L, LC, sg, K, src, ec, cw, x, skip, pin, r, Hook{});
+      launch(k_sm_q<DIM, SM_ADD, false>, quad_wave<DIM>((const void*)k_sm_q<DIM, SM_ADD, false>, sg), T,
+             0, st, L, LC, sg, K, src, ec, cw, x, skip, pin, r, Hook{});
   } else {
     LevelOps<DIM, 1>::sm(M, LC, K, first, src, ec, cw, x, skip, pin, r, hook, st);
   }
@@ -1137,7 +1175,7 @@ int enqueue_cycle(const MgHierarchy& H, const MgWeights& W, const float* r0, flo
   }
   if (cf < H.levels) {
     const CoarsePlan P = coarse_plan(H, W);
-    k_coarse<DIM><<<1, kCoarseThreads, H.coarse_smem, st>>>(P);
+    launch(k_coarse<DIM>, 1, kCoarseThreads, H.coarse_smem, st, P);
     ++launches;
   }
   for (int l = cf - 1; l >= 0; --l) {
@@ -1184,6 +1222,7 @@ __global__ void __launch_bounds__(kT, 2) k_fcg_init(OpView<double> A, Seg sg, Fc
                                                     double* __restrict__ r, float* __restrict__ r32,
                                                     double* partials, double* hist, int64_t hcap,
                                                     Loop h) {
+  pdl_enter();
   constexpr int TX = Tile<DIM>::TX, TY = Tile<DIM>::TY;
   __shared__ double buf[2][Rows<TY>::N][TX * CX + 2];
   const double* __restrict__ b = S->b;
@@ -1234,6 +1273,7 @@ __global__ void __launch_bounds__(kT, 2) k_fcg_dir(OpView<double> A, Seg sg, Fcg
                                                    double* P1, double* __restrict__ q,
                                                    const double* __restrict__ r, double* partials,
                                                    Loop h) {
+  pdl_enter();
   constexpr int TX = Tile<DIM>::TX, TY = Tile<DIM>::TY;
   __shared__ double buf[2][Rows<TY>::N][TX * CX + 2];
   if (S->done) return;
@@ -1284,6 +1324,7 @@ __global__ void k_fcg_update(int64_t n, FcgState* S, double* __restrict__ r,
                              float* __restrict__ r32, const double* P0, const double* P1,
                              const double* __restrict__ q, double* partials, double* hist,
                              int64_t hcap, Loop h) {
+  pdl_enter();
   if (S->done) return;
   const long long it = S->it;
   const double alpha = S->alpha;
@@ -1484,15 +1525,15 @@ int64_t partial_slots(const FineOperator&) { return std::max(kMaxBlocks, 148 * 3
 template <int DIM, int CX>
 void launch_init_t(LearnedSolver* s, const FineOperator& op, Loop h, cudaStream_t st) {
   const Seg sg = make_seg<DIM, CX>(op.A.nx, op.A.ny, op.A.nz);
-  k_fcg_init<DIM, CX><<<seg_grid(sg), kT, 0, st>>>(op.A, sg, s->S, s->r, s->r32, s->partials,
-                                                   s->hist, s->hist_cap, h);
+  launch(k_fcg_init<DIM, CX>, seg_grid(sg), kT, 0, st, op.A, sg, s->S, s->r, s->r32, s->partials,
+         s->hist, s->hist_cap, h);
 }
 
 template <int DIM, int CX>
 void launch_dir_t(LearnedSolver* s, const FineOperator& op, Loop h, cudaStream_t st) {
   const Seg sg = make_seg<DIM, CX>(op.A.nx, op.A.ny, op.A.nz);
-  k_fcg_dir<DIM, CX><<<seg_grid(sg), kT, 0, st>>>(op.A, sg, s->S, s->z32, s->p0, s->p1, s->q, s->r,
-                                                  s->partials, h);
+  launch(k_fcg_dir<DIM, CX>, seg_grid(sg), kT, 0, st, op.A, sg, s->S, s->z32, s->p0, s->p1, s->q,
+         s->r, s->partials, h);
 }
 
 void launch_init(LearnedSolver* s, const FineOperator& op, Loop h, cudaStream_t st) {
@@ -1504,16 +1545,16 @@ template <int DIM>
 [[maybe_unused]] void launch_dir_v(LearnedSolver* s, const FineOperator& op, Loop h, cudaStream_t st) {
   const int64_t nq = (int64_t)(op.A.nx / 4) * op.A.ny * op.A.nz;
   const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((nq + 255) / 256, kGridCap));
-  k_fcg_dir_v<DIM><<<grid, 256, 0, st>>>(op.A, s->S, s->z32, s->p0, s->p1, s->q, s->r,
-                                         s->partials, h);
+  launch(k_fcg_dir_v<DIM>, grid, 256, 0, st, op.A, s->S, s->z32, s->p0, s->p1, s->q, s->r,
+         s->partials, h);
 }
 
 template <int DIM>
 void launch_dir_q(LearnedSolver* s, const FineOperator& op, Loop h, cudaStream_t st) {
   const Seg sg = make_quad_seg<DIM>(op.A.nx, op.A.ny, op.A.nz);
   const int grid = quad_grid<DIM>(sg, (int64_t)dir_blocks_per_sm<DIM>() * 148);
-  k_fcg_dir_q<DIM><<<grid, Quad<DIM>::TX * Quad<DIM>::TY, 0, st>>>(
-      op.A, sg, s->S, s->z32, s->p0, s->p1, s->q, s->r, s->partials, h);
+  launch(k_fcg_dir_q<DIM>, grid, Quad<DIM>::TX * Quad<DIM>::TY, 0, st, op.A, sg, s->S, s->z32,
+         s->p0, s->p1, s->q, s->r, s->partials, h);
 }
 
 void launch_dir(LearnedSolver* s, const FineOperator& op, Loop h, cudaStream_t st) {
@@ -1536,8 +1577,8 @@ int enqueue_body(LearnedSolver* s, const FineOperator& op, Loop h, cudaStream_t 
   const int nv = op.dim == 2 ? enqueue_cycle<2>(*s->H, s->W, s->r32, s->z32, skip, &hk, st)
                              : enqueue_cycle<3>(*s->H, s->W, s->r32, s->z32, skip, &hk, st);
   launch_dir(s, op, h, st);
-  k_fcg_update<<<flat_grid(s->cells), 256, 0, st>>>(s->cells, s->S, s->r, s->r32, s->p0, s->p1,
-                                                    s->q, s->partials, s->hist, s->hist_cap, h);
+  launch(k_fcg_update, flat_grid(s->cells), 256, 0, st, s->cells, s->S, s->r, s->r32, s->p0,
+         s->p1, s->q, s->partials, s->hist, s->hist_cap, h);
   return nv + 2;
 }
 

@@ -153,6 +153,7 @@ __global__ void __launch_bounds__(Quad<DIM>::TX* Quad<DIM>::TY, DIM == 3 ? 4 : 0
     k_res_q(LV L, LV C, Seg sg, const float* __restrict__ x, const float* __restrict__ ec, float cw,
             const float* __restrict__ r, float* __restrict__ res, float* __restrict__ rc,
             int64_t skip) {
+  pdl_enter();
   constexpr int TX = Quad<DIM>::TX, TY = Quad<DIM>::TY, PX = 4 * TX;
   __shared__ __align__(16) float buf[2][Rows<TY>::N][PX + 8];
   __shared__ float2 rows[TY][TX];
@@ -237,6 +238,7 @@ __global__ void __launch_bounds__(Quad<DIM>::TX* Quad<DIM>::TY)
     k_sm_q(LV L, LV C, Seg sg, Kern K, const float* __restrict__ src, const float* __restrict__ ec,
            float cw, float* __restrict__ x, int64_t skip, int64_t pin, const float* __restrict__ r,
            Hook hk) {
+  pdl_enter();
   constexpr int TX = Quad<DIM>::TX, TY = Quad<DIM>::TY, PX = 4 * TX, R0 = Rows<TY>::R0;
   constexpr int NR = Rows<TY>::N;
   __shared__ __align__(16) float ring[3][NR][PX + 8];
@@ -363,6 +365,7 @@ __global__ void __launch_bounds__(Quad<DIM>::TX* Quad<DIM>::TY, dir_blocks_per_s
     k_fcg_dir_q(OpView<double> A, Seg sg, FcgState* S, const float* __restrict__ z, double* P0,
                 double* P1, double* __restrict__ q, const double* __restrict__ r, double* partials,
                 Loop h) {
+  pdl_enter();
   constexpr int TX = Quad<DIM>::TX, TY = Quad<DIM>::TY, PX = 4 * TX;
   __shared__ __align__(16) double buf[2][Rows<TY>::N][PX + 8];
   if (S->done) return;
@@ -476,6 +479,7 @@ __global__ void __launch_bounds__(256) k_fcg_dir_v(OpView<double> A, FcgState* S
                                                    double* P1, double* __restrict__ q,
                                                    const double* __restrict__ r, double* partials,
                                                    Loop h) {
+  pdl_enter();
   if (S->done) return;
   const long long it = S->it;
   const bool first = (it == 0);
