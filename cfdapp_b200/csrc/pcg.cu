@@ -47,8 +47,8 @@ struct cfdb_poperator {
   double* f64[3] = {nullptr, nullptr, nullptr};
   float* f32[3] = {nullptr, nullptr, nullptr};
   // work vectors, allocated on first solve
-  double* w64[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};  // r p0 p1 xalt b x (host staging)
-  float* w32[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};   // r p0 p1 e b32
+  double* w64[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};  // r p0 p1 xalt b x (host staging) z
+  float* w32[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};   // r p0 p1 e b32 z
   double* hist_dev = nullptr;
   int64_t hist_cap = 0;
   double* invd64 = nullptr;  // 1/diag, face-coefficient operators only
@@ -94,6 +94,7 @@ struct PcgParams {
   T* r;
   T* p0;
   T* p1;
+  T* z;  // D^-1 r, written by the TMA kernel's residual sweeps for its next direction sweep
   int x0_zero;
   double abs_tol, rel_tol;
   int64_t max_it;
@@ -455,7 +456,7 @@ cfdb_status launch_pcg_tma(cfdb_context* ctx, PcgParams<T>& P) {
   const uint32_t* halo = S::D3 ? halo3 : halo2;
   const uint32_t* intr = S::D3 ? intr3 : intr2;
   const int es = (int)sizeof(T);
-  if (!encode_tensor_map(&TP.maps.r_halo, dt, es, rank, P.r, dims, halo) ||
+  if (!encode_tensor_map(&TP.maps.z_halo, dt, es, rank, P.z, dims, halo) ||
       !encode_tensor_map(&TP.maps.p0_halo, dt, es, rank, P.p0, dims, halo) ||
       !encode_tensor_map(&TP.maps.p1_halo, dt, es, rank, P.p1, dims, halo) ||
       !encode_tensor_map(&TP.maps.x_int, dt, es, rank, P.x, dims, intr) ||
@@ -492,9 +493,14 @@ cfdb_status launch_pcg_tma(cfdb_context* ctx, PcgParams<T>& P) {
   return CFDB_OK;
 }
 
+// The TMA kernel needs rows that start on 16-byte boundaries.
+bool pcg_uses_tma(const cfdb_poperator* op, size_t word) {
+  return ((int64_t)op->knx * (int64_t)word) % 16 == 0 && !getenv_flag("CFDB_NO_TMA");
+}
+
 template <typename T>
 cfdb_status run_pcg(cfdb_context* ctx, const cfdb_poperator* op, const T* b, T* x, T* r, T* p0,
-                    T* p1, int x0_zero, double abs_tol, double rel_tol, int64_t max_it,
+                    T* p1, T* z, int x0_zero, double abs_tol, double rel_tol, int64_t max_it,
                     double* hist_dev, int64_t hist_cap) {
   PcgParams<T> P{};
   P.A = view<T>(op);
@@ -504,13 +510,14 @@ cfdb_status run_pcg(cfdb_context* ctx, const cfdb_poperator* op, const T* b, T* 
   P.r = r;
   P.p0 = p0;
   P.p1 = p1;
+  P.z = z;
   P.x0_zero = x0_zero;
   P.abs_tol = abs_tol;
   P.rel_tol = rel_tol;
   P.max_it = max_it;
   P.hist = hist_dev;
   P.hist_cap = hist_cap;
-  if (((int64_t)op->knx * (int64_t)sizeof(T)) % 16 == 0 && !getenv_flag("CFDB_NO_TMA")) {
+  if (pcg_uses_tma(op, sizeof(T))) {
     if (is3d(op)) {
       P.cs = make_split<TmaTile3D<T>>(op->knx, op->kny, op->knz);
       return launch_pcg_tma<T, TmaTile3D<T>>(ctx, P);
@@ -529,13 +536,16 @@ cfdb_status run_pcg(cfdb_context* ctx, const cfdb_poperator* op, const T* b, T* 
 // Algorithmic bytes of one persistent PCG launch: the initial pass reads b
 // (and x0) and writes r; each iteration moves 8 vector words per cell (sweep
 // A: r, p_old in, p out; sweep B: x, r, p in, x, r out) plus, with per-face
-// coefficients, the face words each sweep reads.
+// coefficients, the face words each sweep reads.  The TMA kernel also writes
+// z = D^-1 r in the initial pass and in sweep B, and sweep A reads z in
+// place of r: one more word per cell in each.
 double pcg_bytes(const cfdb_poperator* op, size_t word, int64_t iterations, bool x0_zero) {
   const double cells = (double)op->cells;
   int face_words = 0;
   for (int q = 0; q < 3; ++q) face_words += op->f64[q] ? 1 : 0;
-  const double init = cells * (x0_zero ? 2.0 : 3.0) * (double)word;
-  const double per_it = cells * (8.0 + 2.0 * face_words) * (double)word;
+  const double zw = pcg_uses_tma(op, word) ? 1.0 : 0.0;
+  const double init = cells * ((x0_zero ? 2.0 : 3.0) + zw) * (double)word;
+  const double per_it = cells * (8.0 + zw + 2.0 * face_words) * (double)word;
   return init + per_it * (double)iterations;
 }
 
@@ -630,13 +640,13 @@ cfdb_status solve_fp64(cfdb_context* ctx, cfdb_poperator* op, const cfdb_linear_
                        const double* b, double* x, bool x0_zero, int64_t hist_cap,
                        cfdb_linear_result* res) {
   const int64_t n = op->cells;
-  for (int q = 0; q < 3; ++q) {
+  for (int q : {0, 1, 2, 6}) {
     cfdb_status st = alloc_vec(ctx, &op->w64[q], n);
     if (st != CFDB_OK) return st;
   }
   cfdb_status st = ensure_hist(ctx, op, std::max<int64_t>(hist_cap, 1));
   if (st != CFDB_OK) return st;
-  st = run_pcg<double>(ctx, op, b, x, op->w64[0], op->w64[1], op->w64[2], x0_zero ? 1 : 0,
+  st = run_pcg<double>(ctx, op, b, x, op->w64[0], op->w64[1], op->w64[2], op->w64[6], x0_zero ? 1 : 0,
                        s->abs_tol, s->rel_tol, s->max_iterations, op->hist_dev, hist_cap);
   if (st != CFDB_OK) return st;
   st = read_scalars(ctx, 8);
@@ -655,7 +665,7 @@ cfdb_status solve_refined(cfdb_context* ctx, cfdb_poperator* op, const cfdb_line
                           const double* b, double* x, int64_t hist_cap, double* hist_host,
                           cfdb_linear_result* res) {
   const int64_t n = op->cells;
-  for (int q = 0; q < 5; ++q) {
+  for (int q = 0; q < 6; ++q) {
     cfdb_status st = alloc_vec(ctx, &op->w32[q], n);
     if (st != CFDB_OK) return st;
   }
@@ -696,7 +706,7 @@ cfdb_status solve_refined(cfdb_context* ctx, cfdb_poperator* op, const cfdb_line
     // inner: A e = r32 from e = 0 in FP32, reduction inner_tol
     const int64_t budget = s->max_iterations - inner_total;
     CFDB_CUDA(ctx, cudaMemsetAsync(e32, 0, sizeof(float) * (size_t)n, ctx->stream));
-    st = run_pcg<float>(ctx, op, b32, e32, r32, op->w32[1], op->w32[2], 1, 0.0, inner_tol,
+    st = run_pcg<float>(ctx, op, b32, e32, r32, op->w32[1], op->w32[2], op->w32[5], 1, 0.0, inner_tol,
                         budget, op->hist_dev, 0);
     if (st != CFDB_OK) return st;
     st = read_scalars(ctx, 8);
@@ -1026,8 +1036,8 @@ void cfdb_poperator_destroy(cfdb_poperator* op) {
     if (!op->faces_borrowed) cudaFree(op->f64[q]);
     cudaFree(op->f32[q]);
   }
-  for (int q = 0; q < 6; ++q) cudaFree(op->w64[q]);
-  for (int q = 0; q < 5; ++q) cudaFree(op->w32[q]);
+  for (int q = 0; q < 7; ++q) cudaFree(op->w64[q]);
+  for (int q = 0; q < 6; ++q) cudaFree(op->w32[q]);
   cudaFree(op->hist_dev);
   cudaFree(op->invd64);
   cudaFree(op->invd32);

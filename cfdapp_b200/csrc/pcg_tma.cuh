@@ -32,7 +32,7 @@ template <typename T>
 using TmaTile3D = TmaShape<T, 32, 8, 12>;
 
 struct alignas(64) TmaMaps {
-  CUtensorMap r_halo, p0_halo, p1_halo, x_int, r_int;
+  CUtensorMap z_halo, p0_halo, p1_halo, x_int, r_int;
 };
 
 template <typename T>
@@ -173,9 +173,11 @@ __global__ void __launch_bounds__(kTmaThreads, 1) pcg_tma(const __grid_constant_
                                xv(i, j + 1, k), xv(i, j, k - 1), xv(i, j, k + 1));
         }
         P.r[idx] = rn;
+        const T zn = cf.inv * rn;
+        P.z[idx] = zn;
         const double rd = (double)rn;
         acc[0] += rd * rd;
-        acc[1] += rd * (double)(cf.inv * rn);
+        acc[1] += rd * (double)zn;
       }
     }
   }
@@ -215,7 +217,7 @@ __global__ void __launch_bounds__(kTmaThreads, 1) pcg_tma(const __grid_constant_
     const CUtensorMap* pold_map = pold_is_p0 ? &TP.maps.p0_halo : &TP.maps.p1_halo;
     const CUtensorMap* pnew_map = pold_is_p0 ? &TP.maps.p1_halo : &TP.maps.p0_halo;
     T* pnew = pold_is_p0 ? P.p1 : P.p0;
-    // ---- sweep A: stage r, p_old halo boxes; p = D^-1 r + beta p_old; Ap; p.Ap
+    // ---- sweep A: stage z = D^-1 r and p_old halo boxes; p = z + beta p_old; Ap; p.Ap
     double pap = 0.0;
     const bool okA = pipeline(
         [&](const Chunk& c, T* base, uint64_t* bar) {
@@ -223,43 +225,23 @@ __global__ void __launch_bounds__(kTmaThreads, 1) pcg_tma(const __grid_constant_
           mbar_arrive_expect_tx(bar, S::BYTES_A);
           const int hx = c.i0 - S::XO, hy = c.j0 - S::OY, hz = c.z0 - 1;
           if constexpr (S::D3) {
-            tma_load_3d(base, &TP.maps.r_halo, hx, hy, hz, bar);
+            tma_load_3d(base, &TP.maps.z_halo, hx, hy, hz, bar);
             tma_load_3d(base + S::HALO_P, pold_map, hx, hy, hz, bar);
           } else {
-            tma_load_2d(base, &TP.maps.r_halo, hx, hz, bar);
+            tma_load_2d(base, &TP.maps.z_halo, hx, hz, bar);
             tma_load_2d(base + S::HALO_P, pold_map, hx, hz, bar);
           }
         },
         [&](const Chunk& c, T* base) {
-          T* rb = base;
+          // p = z + beta p_old is formed where it is read, by the same fma
+          // everywhere, so each value equals the one stored; outside the
+          // domain both boxes hold the TMA fill 0 and so does p
+          const T* zb = base;
           const T* pb = base + S::HALO_P;
+          auto pv = [&](int e) { return first ? zb[e] : fma(tbeta, pb[e], zb[e]); };
           const int zl = c.z1 - c.z0;
           constexpr int PL = S::HX * S::HY;  // box plane stride
-          // transform p = D^-1 r + beta p_old over the used halo elements
-          // (columns XO-1 .. XO+TX of the box), evenly over the threads
-          constexpr int UX = S::TX + 2;
-          const int nuse = UX * S::HY * (zl + 2);
-          for (int u = tid; u < nuse; u += kTmaThreads) {
-            const int cx = u % UX;
-            const int rest = u / UX;
-            const int cy = rest % S::HY, kk = rest / S::HY - 1;
-            const int i = c.i0 - 1 + cx, j = c.j0 - S::OY + cy, k = c.z0 + kk;
-            if (i < 0 || i >= A.nx || j < 0 || j >= A.ny || k < 0 || k >= A.nz) continue;
-            const int e = (cx + S::XO - 1) + S::HX * cy + PL * (kk + 1);
-            T inv;
-            if constexpr (FACE) {
-              inv = __ldg(P.invd + (i + (int64_t)A.nx * (j + (int64_t)A.ny * k)));
-            } else {
-              const T sxy = ((__ldg(A.tx + i) + __ldg(A.tx + i + 1)) + __ldg(A.ty + j)) + __ldg(A.ty + j + 1);
-              const T dg = (sxy + __ldg(A.tz + k)) + __ldg(A.tz + k + 1);
-              const bool pin = A.pinned && (i + (int64_t)A.nx * (j + (int64_t)A.ny * k)) == A.ref;
-              inv = pin ? T(1) : rcp_rn(dg);
-            }
-            const T z = inv * rb[e];
-            rb[e] = first ? z : fma(tbeta, pb[e], z);
-          }
-          __syncthreads();
-          // interior: Ap, store p, p.Ap -- one thread per column (x fastest)
+          // one thread per column (x fastest), z neighbours carried in registers
           constexpr int ICOL = S::TX * S::TY;
           constexpr int SPLIT = kTmaThreads / ICOL > 0 ? kTmaThreads / ICOL : 1;
           for (int t = tid; t < ICOL * SPLIT; t += kTmaThreads) {
@@ -271,38 +253,43 @@ __global__ void __launch_bounds__(kTmaThreads, 1) pcg_tma(const __grid_constant_
             int e = (qx + S::XO) + S::HX * (qy + S::OY) + PL * (kb + 1);
             int64_t idx = i + (int64_t)A.nx * (j + (int64_t)A.ny * (c.z0 + kb));
             const int64_t pstride = (int64_t)A.nx * A.ny;
+            T lo = pv(e - PL), v = pv(e);
             if constexpr (FACE) {
               for (int kk = kb; kk < ke; ++kk, e += PL, idx += pstride) {
+                const T hi = pv(e + PL);
                 const Coef<T> cf = face_coef(A, i, j, c.z0 + kk);
-                const T v = rb[e];
-                const T ap = apply_coef(cf, v, rb[e - 1], rb[e + 1], S::D3 ? rb[e - S::HX] : T(0),
-                                        S::D3 ? rb[e + S::HX] : T(0), rb[e - PL], rb[e + PL]);
+                const T ap = apply_coef(cf, v, pv(e - 1), pv(e + 1), S::D3 ? pv(e - S::HX) : T(0),
+                                        S::D3 ? pv(e + S::HX) : T(0), lo, hi);
                 pnew[idx] = v;
                 pap += (double)v * (double)ap;
+                lo = v;
+                v = hi;
               }
             } else {
               const ColCoef<T> cc = column_coef(A, i, j);
               for (int kk = kb; kk < ke; ++kk, e += PL, idx += pstride) {
                 const int k = c.z0 + kk;
+                const T hi = pv(e + PL);
                 const T zl_ = __ldg(A.tz + k), zh_ = __ldg(A.tz + k + 1);
-                const T v = rb[e];
                 T ap;
                 if (cc.has_ref && k == cc.ref_k) {
                   ap = v;
                 } else {
                   const T dg = (cc.sxy + zl_) + zh_;
-                  T off = cc.cxl * rb[e - 1];
-                  off = fma(cc.cxh, rb[e + 1], off);
+                  T off = cc.cxl * pv(e - 1);
+                  off = fma(cc.cxh, pv(e + 1), off);
                   if (S::D3) {
-                    off = fma(cc.cyl, rb[e - S::HX], off);
-                    off = fma(cc.cyh, rb[e + S::HX], off);
+                    off = fma(cc.cyl, pv(e - S::HX), off);
+                    off = fma(cc.cyh, pv(e + S::HX), off);
                   }
-                  off = fma(k > 0 ? zl_ : T(0), rb[e - PL], off);
-                  off = fma(k < A.nz - 1 ? zh_ : T(0), rb[e + PL], off);
+                  off = fma(k > 0 ? zl_ : T(0), lo, off);
+                  off = fma(k < A.nz - 1 ? zh_ : T(0), hi, off);
                   ap = fma(dg, v, -off);
                 }
                 pnew[idx] = v;
                 pap += (double)v * (double)ap;
+                lo = v;
+                v = hi;
               }
             }
           }
@@ -327,7 +314,8 @@ __global__ void __launch_bounds__(kTmaThreads, 1) pcg_tma(const __grid_constant_
       return;
     }
     const T talpha = (T)alpha;
-    // ---- sweep B: stage p halo, x and r interiors; x += alpha p; r -= alpha A p
+    // ---- sweep B: stage p halo, x and r interiors; x += alpha p; r -= alpha A p;
+    // z = D^-1 r stored for the next sweep A
     double ab[2] = {0.0, 0.0};
     const bool okB = pipeline(
         [&](const Chunk& c, T* base, uint64_t* bar) {
@@ -394,9 +382,11 @@ __global__ void __launch_bounds__(kTmaThreads, 1) pcg_tma(const __grid_constant_
               P.x[idx] = fma(talpha, v, xb[q]);
               const T rn = fma(-talpha, ap, rb[q]);
               P.r[idx] = rn;
+              const T zn = inv * rn;
+              P.z[idx] = zn;
               const double rd = (double)rn;
               ab[0] += rd * rd;
-              ab[1] += rd * (double)(inv * rn);
+              ab[1] += rd * (double)zn;
             }
           }
         });
