@@ -1,13 +1,17 @@
 // Allocation-free p' solve.
 //
 // Some callers cannot allocate device memory at the point where they need a
-// solve: code running inside a CUDA stream capture that must not add memory
-// nodes, hosts whose allocator is owned by another runtime (an embedding
-// application or FFI host that hands us pre-registered buffers), or real-time
-// loops that forbid cudaMalloc/cudaFree after start-up.  For them,
-// cfdb_pcg_solve_noalloc runs the FP64 Jacobi-PCG of the uniform p' operator
-// using only the caller's b and x plus the fixed scratch array below; it
-// creates no context, stream, event or allocation.
+// solve: hosts whose device memory is owned by another runtime (an embedding
+// application or FFI host that hands us pre-registered buffers and reserves
+// the rest of the device for its own pool), or real-time loops that forbid
+// cudaMalloc/cudaFree after start-up (both synchronise the device and can
+// stall).  For them, cfdb_pcg_solve_noalloc runs the FP64 Jacobi-PCG of the
+// uniform p' operator using only the caller's b and x plus the fixed scratch
+// array below; it creates no context, stream, event or allocation.  It does
+// wait for its own result (a stream synchronisation), so it cannot be
+// recorded into a CUDA graph: on a capturing stream it returns
+// CFDB_ERR_UNSUPPORTED before it issues any work, and the capture stays
+// valid.
 //
 // The scratch is one file-scope device array of kScratchBytes (about 1.6 MB)
 // that every GPU which loads this library holds until the process exits.  It
@@ -202,20 +206,48 @@ __global__ void __launch_bounds__(kNaThreads) na_pcg(NaParams P) {
   finish(CFDB_SOLVER_MAX_ITERATIONS, P.max_it, res_cur);
 }
 
-// Device address of the scratch array, looked up once per device.
+// Device address of the scratch array.  In host code g_noalloc_scratch names
+// a host-side stand-in, not device memory, so the kernel gets the address
+// cudaGetSymbolAddress returns, looked up once per device and CUDA context
+// with that device current.  The cache is keyed on the context as well as the
+// device: after cudaDeviceReset the primary context (and the library's module
+// with its array) is created anew, and an address of the old one would
+// dangle.  cuCtxGetCurrent is reached through the runtime's driver entry
+// point, so the library does not link the driver library itself.
+using CtxGetCurrentFn = int (*)(void**);
+
 std::mutex g_lookup_mutex;
-void* g_scratch_addr[128] = {};
+struct ScratchSlot {
+  void* context = nullptr;
+  void* addr = nullptr;
+};
+ScratchSlot g_scratch_slot[128];
+CtxGetCurrentFn g_ctx_get_current = nullptr;
+bool g_ctx_lookup_done = false;
 
 cudaError_t scratch_address(int device, unsigned char** out) {
   std::lock_guard<std::mutex> lock(g_lookup_mutex);
   if (device < 0 || device >= 128) return cudaErrorInvalidDevice;
-  if (!g_scratch_addr[device]) {
+  if (!g_ctx_lookup_done) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      g_ctx_get_current = reinterpret_cast<CtxGetCurrentFn>(fn);
+    g_ctx_lookup_done = true;
+  }
+  void* context = nullptr;
+  if (!g_ctx_get_current || g_ctx_get_current(&context) != 0 || !context)
+    return cudaErrorDeviceUninitialized;
+  ScratchSlot& slot = g_scratch_slot[device];
+  if (!slot.addr || slot.context != context) {
     void* p = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess) return e;
-    g_scratch_addr[device] = p;
+    slot.addr = p;
+    slot.context = context;
   }
-  *out = static_cast<unsigned char*>(g_scratch_addr[device]);
+  *out = static_cast<unsigned char*>(slot.addr);
   return cudaSuccess;
 }
 
@@ -241,11 +273,17 @@ extern "C" cfdb_status cfdb_pcg_solve_noalloc(void* stream, const cfdb_grid* gri
       s->precision != CFDB_PRECISION_FP64 || s->max_iterations < 1 || !(rho > 0.0))
     return CFDB_ERR_UNSUPPORTED;
   if (pinned && (reference_cell < 0 || reference_cell >= cells)) return CFDB_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = (cudaStream_t)stream;
+  // the call waits for its own result, which a capturing stream forbids:
+  // refuse before any other CUDA call so that the caller's capture survives
+  cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &capture) != cudaSuccess ||
+      capture != cudaStreamCaptureStatusNone)
+    return CFDB_ERR_UNSUPPORTED;
   int device = 0;
   if (cudaGetDevice(&device) != cudaSuccess) return CFDB_ERR_NO_DEVICE;
   unsigned char* scratch = nullptr;
   if (scratch_address(device, &scratch) != cudaSuccess) return CFDB_ERR_CUDA;
-  cudaStream_t st = (cudaStream_t)stream;
 
   NaParams P{};
   NaGrid& G = P.G;
@@ -310,7 +348,11 @@ extern "C" cfdb_status cfdb_pcg_solve_noalloc(void* stream, const cfdb_grid* gri
           cudaSuccess ||
       cudaStreamSynchronize(st) != cudaSuccess)
     return CFDB_ERR_CUDA;
-  if (sync_words[2] != 0) return CFDB_ERR_DEVICE_TIMEOUT;
+  if (sync_words[2] != 0) {
+    // x_dev holds a partial iterate: undefined as a solution or a start
+    result->iterations = (int64_t)out[1];
+    return CFDB_ERR_DEVICE_TIMEOUT;
+  }
   result->status = (int)out[0];
   result->iterations = (int64_t)out[1];
   result->initial_residual = out[2];

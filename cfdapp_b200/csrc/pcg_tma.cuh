@@ -129,7 +129,10 @@ __global__ void __launch_bounds__(kTmaThreads, 1) pcg_tma(const __grid_constant_
   auto idx_of = [&](int i, int j, int k) { return i + (int64_t)A.nx * (j + (int64_t)A.ny * k); };
 
   // Generic pipelined sweep: load(c, base, bar) issues the chunk's TMA copies
-  // (thread 0), body(c, base) computes it.  Returns false on a failed wait.
+  // (thread 0), body(c, base) computes it.  Returns false on a failed wait;
+  // before that, thread 0 waits (bounded) for the copies still in flight in
+  // either stage, so that the block leaves no bulk copy writing its shared
+  // memory behind.
   auto pipeline = [&](auto load, auto body) -> bool {
     SlabIter ld{blk}, cp{blk};
     Chunk cl, cc;
@@ -139,11 +142,18 @@ __global__ void __launch_bounds__(kTmaThreads, 1) pcg_tma(const __grid_constant_
     while (cp.template next<S::TZ>(cs, A.nz, S::TX, S::TY, B, cc)) {
       const int st = q & 1;
       Chunk cn;
-      if (ld.template next<S::TZ>(cs, A.nz, S::TX, S::TY, B, cn) && tid == 0)
+      const bool issued = ld.template next<S::TZ>(cs, A.nz, S::TX, S::TY, B, cn);
+      if (issued && tid == 0)
         load(cn, stage_mem + (size_t)(st ^ 1) * S::STAGE, &bars[st ^ 1]);
       const bool ok = mbar_wait(&bars[st], parity[st], P.sync.error, P.sync.timeout_ns);
+      if (__syncthreads_or(!ok)) {
+        if (tid == 0) {
+          if (!ok) mbar_drain(&bars[st], parity[st], P.sync.timeout_ns);
+          if (issued) mbar_drain(&bars[st ^ 1], parity[st ^ 1], P.sync.timeout_ns);
+        }
+        return false;
+      }
       parity[st] ^= 1u;
-      if (__syncthreads_or(!ok)) return false;
       body(cc, stage_mem + (size_t)st * S::STAGE);
       __syncthreads();
       ++q;

@@ -69,6 +69,17 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, unsign
   return true;
 }
 
+// Bounded wait on phase `parity` of `bar` that ignores the error flag: a
+// block that gives up on an error first lets the bulk copies it issued into
+// its shared memory land, so that none is still writing when the block
+// exits.  Returns at the latest after timeout_ns.
+__device__ __forceinline__ void mbar_drain(uint64_t* bar, uint32_t parity,
+                                           unsigned long long timeout_ns) {
+  const unsigned long long t0 = global_ns();
+  while (!mbar_try_wait(bar, parity))
+    if (global_ns() - t0 > timeout_ns) return;
+}
+
 // Orders this thread's earlier generic-proxy accesses of shared memory before
 // subsequent async-proxy (TMA) writes to it.
 __device__ __forceinline__ void fence_proxy_async_smem() {

@@ -460,19 +460,25 @@ CFDB_API cfdb_status cfdb_selftest_wait_timeout(cfdb_context* ctx, double timeou
 /* No counterpart in the reference.  The FP64 Jacobi-PCG of the uniform p'
  * operator (the system cfdb_poperator_create_uniform builds with no
  * Dirichlet patch) for callers that cannot allocate device memory when they
- * solve -- inside a stream capture that must not add allocations, under an
- * allocator owned by another runtime, or in a loop that forbids
- * cudaMalloc/cudaFree after start-up.  It needs no context: it launches on
+ * solve -- a host whose device memory belongs to another runtime's
+ * allocator, or a loop that forbids cudaMalloc/cudaFree after start-up
+ * (both synchronise the device).  It needs no context: it launches on
  * `stream` (NULL: the legacy default stream) of the current device, reads
  * b_dev, updates x_dev (x0 on entry), and keeps every other vector and
  * reduction slot in one fixed device array of about 1.6 MB that each GPU
  * loading this library holds until exit.  Grids above 65536 cells return
  * CFDB_ERR_UNSUPPORTED, as do settings other than CG + Jacobi in FP64.
- * The first call on each device looks the array's address up
- * (cudaGetSymbolAddress); make that first call outside any stream capture.
- * Every call clears what must start at zero, but all calls share the array:
- * calls whose work overlaps on the GPU race on it.  Fills status,
- * iterations, initial and final residual of `result`; no timing. */
+ * The call waits for its result (it synchronises `stream`), so it cannot be
+ * recorded into a CUDA graph: on a capturing stream it returns
+ * CFDB_ERR_UNSUPPORTED before issuing any work and the capture stays valid.
+ * The first call on each device (and again after the device's context is
+ * re-created, e.g. by cudaDeviceReset) looks the array's address up with
+ * cudaGetSymbolAddress.  Every call clears what must start at zero, but all
+ * calls share the array: calls whose work overlaps on the GPU race on it.
+ * Fills status, iterations, initial and final residual of `result`; no
+ * timing.  After CFDB_ERR_DEVICE_TIMEOUT (a bounded device-side wait gave
+ * up) x_dev holds a partial iterate, undefined as a solution or as a start;
+ * result->iterations then tells how far the solve got. */
 CFDB_API cfdb_status cfdb_pcg_solve_noalloc(void* stream, const cfdb_grid* grid, double rho,
                                             int pinned, int64_t reference_cell,
                                             const cfdb_linear_settings* settings,
