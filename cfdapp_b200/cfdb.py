@@ -926,3 +926,107 @@ def _batch_write_results(self, k: int, directory: str) -> bool:
 
 Simple.write_results = _simple_write_results
 Batch.write_results = _batch_write_results
+
+
+# ------------------------------------------------------------------ CSR systems
+CSR_PATH = {0: "stencil", 1: "faces"}
+
+
+class _CsrInfo(C.Structure):
+    _fields_ = [("dim", C.c_int), ("n", C.c_int64 * 3), ("path", C.c_int),
+                ("faces_eligible", C.c_int), ("pinned", C.c_int), ("reference_cell", C.c_int64),
+                ("learned_declined", C.c_int)]
+
+    def as_dict(self) -> dict:
+        return {"dim": self.dim, "n": tuple(self.n[: self.dim]), "path": CSR_PATH[self.path],
+                "faces_eligible": bool(self.faces_eligible), "pinned": bool(self.pinned),
+                "reference_cell": int(self.reference_cell),
+                "learned_declined": bool(self.learned_declined)}
+
+
+def _csr_sigs(L):
+    if getattr(L, "_csr_sigs", False):
+        return
+    vp, i64, dbl = C.c_void_p, C.c_int64, C.c_double
+    u64p = C.POINTER(C.c_uint64)
+    L.cfdb_csr_analyze.argtypes = [i64, u64p, u64p, C.POINTER(dbl), C.POINTER(_CsrInfo)]
+    L.cfdb_csr_solver_create.argtypes = [vp, C.POINTER(vp)]
+    L.cfdb_csr_solver_destroy.argtypes = [vp]
+    L.cfdb_csr_solver_destroy.restype = None
+    L.cfdb_csr_solve_host.argtypes = [vp, C.POINTER(_LinSettings), i64, u64p, u64p, C.POINTER(dbl),
+                                      C.POINTER(dbl), C.POINTER(dbl), C.POINTER(dbl), i64,
+                                      C.POINTER(_LinResult), C.POINTER(_CsrInfo)]
+    L._csr_sigs = True
+
+
+def _csr_arrays(offsets, columns, values):
+    ro = np.ascontiguousarray(offsets, dtype=np.uint64)
+    ci = np.ascontiguousarray(columns, dtype=np.uint64)
+    v = np.ascontiguousarray(values, dtype=np.float64)
+    return ro, ci, v
+
+
+def csr_analyze(offsets, columns, values) -> dict | None:
+    """cfdb_csr_analyze: the recognised grid and path of a CSR matrix, or
+    None when it is not a structured 5-/7-point operator (host only)."""
+    L = load()
+    _csr_sigs(L)
+    ro, ci, v = _csr_arrays(offsets, columns, values)
+    info = _CsrInfo()
+    u64p = C.POINTER(C.c_uint64)
+    st = L.cfdb_csr_analyze(len(ro) - 1, ro.ctypes.data_as(u64p), ci.ctypes.data_as(u64p), _dp(v),
+                            C.byref(info))
+    if st == -6:
+        return None
+    if st != CFDB_OK:
+        raise CfdbError(f"cfdb_csr_analyze: {ERRORS.get(st, st)}")
+    return info.as_dict()
+
+
+class CsrSolver:
+    """cfdb_csr_solver: solves of the reference's CSR LinearSystem."""
+
+    def __init__(self, ctx: Context):
+        self.ctx = ctx
+        _csr_sigs(ctx.lib)
+        h = C.c_void_p()
+        ctx.check(ctx.lib.cfdb_csr_solver_create(ctx.handle, C.byref(h)), "cfdb_csr_solver_create")
+        self._h = h
+        self.info = None
+
+    def solve(self, offsets, columns, values, b, settings: LinearSolverSettings,
+              x0=None, history_cap: int | None = None) -> SolverResult:
+        ro, ci, v = _csr_arrays(offsets, columns, values)
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.zeros(len(b)) if x0 is None else np.array(x0, dtype=np.float64)
+        cap = (settings.max_iterations + 1) if history_cap is None else history_cap
+        hist = np.zeros(max(cap, 1))
+        res = _LinResult()
+        info = _CsrInfo()
+        cs = settings.c()
+        u64p = C.POINTER(C.c_uint64)
+        self.ctx.check(self.ctx.lib.cfdb_csr_solve_host(
+            self._h, C.byref(cs), len(ro) - 1, ro.ctypes.data_as(u64p), ci.ctypes.data_as(u64p),
+            _dp(v), _dp(b), _dp(x), _dp(hist), cap, C.byref(res), C.byref(info)),
+            "cfdb_csr_solve_host")
+        self.info = info.as_dict() if info.dim else None
+        if cs.preconditioner == PRECOND["learned_mg"] and self.info and self.info["path"] == "faces":
+            m = res.iterations - res.fallback_iterations + 1
+        else:
+            m = res.iterations + 1
+        m = min(cap, m) if res.status not in (3, 5) else 0
+        return SolverResult(SOLVER_STATUS[res.status], res.iterations, res.initial_residual,
+                            res.final_residual, res.true_residual, res.refinements, res.restarts,
+                            res.device_ms, res.kernel_launches, res.krylov_ms, res.krylov_bytes,
+                            res.krylov_launches, res.fallback_iterations, hist[:m].copy(), x)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.ctx.lib.cfdb_csr_solver_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

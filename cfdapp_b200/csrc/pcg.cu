@@ -953,6 +953,50 @@ void poperator_learned(cfdb_poperator* op, FineOperator* fo, LearnedSolver** sol
   *version = op->version;
 }
 
+// Copies host face coefficients (global face order) into the operator's own
+// FP64/FP32 face arrays (allocated when `alloc`), refreshes the inverse
+// diagonals and bumps the coefficient version, so that a learned solve
+// refreshes its hierarchy's values instead of rebuilding it.
+cfdb_status upload_faces(cfdb_context* ctx, cfdb_poperator* op, const double* face_coeff_host,
+                         bool alloc) {
+  const cfdb_grid& g = op->grid;
+  const int64_t nx = g.n[0], ny = g.n[1], nz = g.dim == 3 ? g.n[2] : 1;
+  const int64_t nfx = (nx + 1) * ny * nz, nfy = nx * (ny + 1) * nz, nfz = g.dim == 3 ? nx * ny * (nz + 1) : 0;
+  const int64_t counts[3] = {nfx, nfy, nfz};
+  const int64_t offs[3] = {0, nfx, nfx + nfy};
+  // real axis -> kernel axis: 2D y-faces become kernel z-faces
+  const int kaxis[3] = {0, g.dim == 2 ? 2 : 1, 2};
+  for (int64_t q = 0; q < nfx + nfy + nfz; ++q)
+    if (!std::isfinite(face_coeff_host[q]))
+      return set_error(ctx, CFDB_ERR_INVALID_ARGUMENT, "non-finite face coefficient");
+  for (int a = 0; a < g.dim; ++a) {
+    const int ka = kaxis[a];
+    const int64_t m = counts[a];
+    std::vector<float> f32(m);
+    for (int64_t q = 0; q < m; ++q) f32[q] = (float)face_coeff_host[offs[a] + q];
+    if (alloc) {
+      cudaError_t e1 = cudaMalloc((void**)&op->f64[ka], m * sizeof(double));
+      cudaError_t e2 = cudaMalloc((void**)&op->f32[ka], m * sizeof(float));
+      if (e1 != cudaSuccess || e2 != cudaSuccess)
+        return set_error(ctx, CFDB_ERR_OUT_OF_MEMORY, "face coefficient allocation failed");
+    }
+    CFDB_CUDA(ctx, cudaMemcpy(op->f64[ka], face_coeff_host + offs[a], m * sizeof(double),
+                              cudaMemcpyHostToDevice));
+    CFDB_CUDA(ctx, cudaMemcpy(op->f32[ka], f32.data(), m * sizeof(float), cudaMemcpyHostToDevice));
+  }
+  if (alloc) {
+    CFDB_CUDA(ctx, cudaMalloc((void**)&op->invd64, sizeof(double) * (size_t)op->cells));
+    CFDB_CUDA(ctx, cudaMalloc((void**)&op->invd32, sizeof(float) * (size_t)op->cells));
+  }
+  inverse_diagonal<double><<<1024, 256, 0, ctx->stream>>>(view<double>(op), op->invd64);
+  inverse_diagonal<float><<<1024, 256, 0, ctx->stream>>>(view<float>(op), op->invd32);
+  CFDB_CHECK_LAUNCH(ctx);
+  count_launch(ctx, 2);
+  ++op->version;
+  CFDB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return CFDB_OK;
+}
+
 }  // namespace cfdb
 
 using namespace cfdb;
@@ -987,45 +1031,24 @@ cfdb_status cfdb_poperator_create_faces(cfdb_context* ctx, const cfdb_grid* grid
   cfdb_status st = new_operator(ctx, grid, pinned, reference_cell, &op);
   if (st != CFDB_OK) return st;
   st = build_tables(ctx, op, 1.0, 0u);  // zero-filled fallbacks for absent axes
+  if (st == CFDB_OK) st = upload_faces(ctx, op, face_coeff_host, true);
   if (st != CFDB_OK) {
     cfdb_poperator_destroy(op);
     return st;
   }
-  const cfdb_grid& g = *grid;
-  const int64_t nx = g.n[0], ny = g.n[1], nz = g.dim == 3 ? g.n[2] : 1;
-  const int64_t nfx = (nx + 1) * ny * nz, nfy = nx * (ny + 1) * nz, nfz = g.dim == 3 ? nx * ny * (nz + 1) : 0;
-  const int64_t counts[3] = {nfx, nfy, nfz};
-  const int64_t offs[3] = {0, nfx, nfx + nfy};
-  // real axis -> kernel axis: 2D y-faces become kernel z-faces
-  const int kaxis[3] = {0, g.dim == 2 ? 2 : 1, 2};
-  for (int a = 0; a < g.dim; ++a) {
-    const int ka = kaxis[a];
-    const int64_t m = counts[a];
-    for (int64_t q = 0; q < m; ++q)
-      if (!std::isfinite(face_coeff_host[offs[a] + q])) {
-        cfdb_poperator_destroy(op);
-        return set_error(ctx, CFDB_ERR_INVALID_ARGUMENT, "non-finite face coefficient");
-      }
-    std::vector<float> f32(m);
-    for (int64_t q = 0; q < m; ++q) f32[q] = (float)face_coeff_host[offs[a] + q];
-    cudaError_t e1 = cudaMalloc((void**)&op->f64[ka], m * sizeof(double));
-    cudaError_t e2 = cudaMalloc((void**)&op->f32[ka], m * sizeof(float));
-    if (e1 != cudaSuccess || e2 != cudaSuccess) {
-      cfdb_poperator_destroy(op);
-      return set_error(ctx, CFDB_ERR_OUT_OF_MEMORY, "face coefficient allocation failed");
-    }
-    CFDB_CUDA(ctx, cudaMemcpy(op->f64[ka], face_coeff_host + offs[a], m * sizeof(double),
-                              cudaMemcpyHostToDevice));
-    CFDB_CUDA(ctx, cudaMemcpy(op->f32[ka], f32.data(), m * sizeof(float), cudaMemcpyHostToDevice));
-  }
-  CFDB_CUDA(ctx, cudaMalloc((void**)&op->invd64, sizeof(double) * (size_t)op->cells));
-  CFDB_CUDA(ctx, cudaMalloc((void**)&op->invd32, sizeof(float) * (size_t)op->cells));
-  inverse_diagonal<double><<<1024, 256, 0, ctx->stream>>>(view<double>(op), op->invd64);
-  inverse_diagonal<float><<<1024, 256, 0, ctx->stream>>>(view<float>(op), op->invd32);
-  CFDB_CHECK_LAUNCH(ctx);
-  CFDB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   *out = op;
   return CFDB_OK;
+}
+
+cfdb_status cfdb_poperator_update_faces(cfdb_context* ctx, cfdb_poperator* op,
+                                        const double* face_coeff_host) {
+  if (!ctx || !op || !face_coeff_host) return CFDB_ERR_INVALID_ARGUMENT;
+  if (op->faces_borrowed || !op->f64[0])
+    return set_error(ctx, CFDB_ERR_INVALID_ARGUMENT,
+                     "the operator holds no face arrays of its own (cfdb_poperator_create_faces "
+                     "makes one that does)");
+  CFDB_CUDA(ctx, cudaSetDevice(ctx->device));
+  return upload_faces(ctx, op, face_coeff_host, false);
 }
 
 void cfdb_poperator_destroy(cfdb_poperator* op) {

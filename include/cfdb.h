@@ -159,6 +159,13 @@ CFDB_API cfdb_status cfdb_poperator_create_uniform(cfdb_context* ctx, const cfdb
 CFDB_API cfdb_status cfdb_poperator_create_faces(cfdb_context* ctx, const cfdb_grid* grid,
                                         const double* face_coeff_host, int pinned,
                                         int64_t reference_cell, cfdb_poperator** out);
+/* New face coefficients for an operator made by _create_faces (same grid,
+ * pinning and layout): the values a SIMPLE host assembles again every outer
+ * iteration (assembleGeometricPressureCorrection, :181-339).  Keeps the
+ * operator's device arrays and, for the learned solve, its hierarchy and
+ * solve graph (only their values are refreshed). */
+CFDB_API cfdb_status cfdb_poperator_update_faces(cfdb_context* ctx, cfdb_poperator* op,
+                                                 const double* face_coeff_host);
 CFDB_API void cfdb_poperator_destroy(cfdb_poperator* op);
 CFDB_API int64_t cfdb_poperator_cells(const cfdb_poperator* op);
 
@@ -181,6 +188,75 @@ CFDB_API cfdb_status cfdb_poperator_solve_host(cfdb_context* ctx, const cfdb_pop
                                       const cfdb_linear_settings* settings, const double* b_host,
                                       double* x_host, double* history, int64_t history_cap,
                                       cfdb_linear_result* result);
+
+/* ------------------------------------------- CSR systems (LinearSystem) */
+
+/* The reference's solver contract takes a host CSR LinearSystem
+ * (include/cfd/algebra/LinearSystem.hpp:12-24, SparseMatrix.hpp:19-56:
+ * row offsets and ascending 64-bit column indices, exact zeros dropped) and
+ * an initial guess, LinearSolver::solve (LinearSolver.hpp:176-180); the GPU
+ * plugin that serves it is cfd::gpu::makeGpuCG / makeGpuBiCGSTAB
+ * (include/cfd/gpu/GpuLinearSolver.hpp:48-54).  These entry points take the
+ * same arrays.
+ *
+ * Recognition: the matrix must be the structured 5-point (2D) or 7-point
+ * (3D) operator of a Cartesian grid in the reference's cell order
+ * (i + nx*(j + ny*k)): every stored off-diagonal couples a cell to a grid
+ * neighbour, and the strides 1, nx (, nx*ny) all occur (a band with stride 1
+ * only is taken as one row of cells, nx x 1).  That is the shape of
+ * every momentum and p' system the reference assembles on createCartesian2D
+ * / createCartesian3D meshes (the wall three-point term couples a wall cell
+ * to its first neighbour, so it stays in the band).  Anything else is
+ * CFDB_ERR_UNSUPPORTED: the library runs no CSR kernel and no CPU solver.
+ *
+ * Paths: a CG system whose couplings are symmetric apart from at most one
+ * identity row (the pinned reference cell, PressureCorrectionEquation.cpp:
+ * 326-329), whose boundary faces carry no coefficient, and whose stored
+ * diagonal equals the face-order sum of its couplings bit for bit is solved
+ * by the face-coefficient p' operator (CFDB_CSR_PATH_FACES: the persistent
+ * Jacobi-PCG, or the learned preconditioner); every other recognised system
+ * (BiCGSTAB, non-symmetric momentum rows, Dirichlet faces, no
+ * preconditioner) by the stencil Krylov solver with the stored diagonal
+ * (CFDB_CSR_PATH_STENCIL).  A learned-preconditioner request on a system that
+ * only the stencil path takes runs Jacobi-PCG and says so in
+ * info->learned_declined. */
+enum { CFDB_CSR_PATH_STENCIL = 0, CFDB_CSR_PATH_FACES = 1 };
+typedef struct {
+  int dim;                 /* 2 or 3 */
+  int64_t n[3];            /* cells per axis (n[2] = 1 in 2D) */
+  int path;                /* CFDB_CSR_PATH_* the solve took (faces_eligible for _analyze) */
+  int faces_eligible;      /* the face-coefficient operator reproduces the matrix exactly */
+  int pinned;              /* one identity row found */
+  int64_t reference_cell;  /* its index (-1 if none) */
+  int learned_declined;    /* LEARNED_MG asked for but the system needs the stencil path */
+} cfdb_csr_info;
+
+/* Host-only recognition (no device needed): fills info or returns
+ * CFDB_ERR_UNSUPPORTED. */
+CFDB_API cfdb_status cfdb_csr_analyze(int64_t rows, const uint64_t* row_offsets,
+                                      const uint64_t* columns, const double* values,
+                                      cfdb_csr_info* info);
+
+typedef struct cfdb_csr_solver cfdb_csr_solver;
+/* A solver keeps its device buffers (and, on the faces path, the operator
+ * with its learned hierarchy) between solves of systems of one shape, as the
+ * reference's GPU solvers keep theirs (GpuLinearSolverCuda.cpp:327-334). */
+CFDB_API cfdb_status cfdb_csr_solver_create(cfdb_context* ctx, cfdb_csr_solver** out);
+CFDB_API void cfdb_csr_solver_destroy(cfdb_csr_solver* s);
+/* Solves A x = b from x0 (x_host in, solution out) with the settings'
+ * Krylov method and preconditioner; statuses, convergence test and
+ * residual history as CG::solve / BiCGSTAB::solve (src/algebra/CG.cpp:14-148,
+ * BiCGSTAB.cpp:48-275): NonFiniteInput for a non-finite value of A, b or x0
+ * (checked first), InvalidSystem when the Jacobi build fails
+ * (Preconditioner.cpp:11-32), then the solve.  history (may be NULL) gets up
+ * to history_cap entries of residualHistory.  info (may be NULL) reports the
+ * recognised grid and the path taken. */
+CFDB_API cfdb_status cfdb_csr_solve_host(cfdb_csr_solver* s, const cfdb_linear_settings* settings,
+                                         int64_t rows, const uint64_t* row_offsets,
+                                         const uint64_t* columns, const double* values,
+                                         const double* b_host, double* x_host, double* history,
+                                         int64_t history_cap, cfdb_linear_result* result,
+                                         cfdb_csr_info* info);
 
 /* Device buffers owned by the context's allocator (for callers without a
  * CUDA runtime of their own: tests, FFI hosts). */

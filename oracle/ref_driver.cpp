@@ -28,12 +28,20 @@
 //       {inlet,0} left, Outlet right, Walls; pressure FixedValue(0) at the
 //       outlet), pressure FixedGradient(0) elsewhere.  Writes u v [w] p flux
 //       and the residual histories.
+//
+//   csr in=DIR [solver=bicgstab|cg] [pre=none|jacobi] [atol=1e-12] [rtol=1e-10]
+//       [maxit=1000] [out=DIR]
+//       a stored CSR LinearSystem (DIR/{offsets,columns}.bin as uint64,
+//       DIR/{values,rhs,x0}.bin as float64) solved by the reference BiCGSTAB
+//       (BiCGSTAB.cpp:48) or CG from the stored initial guess; writes the
+//       solution and the residual history.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <fstream>
+#include <stdexcept>
 #include <map>
 #include <memory>
 #include <string>
@@ -389,11 +397,67 @@ int runSimple(const Args& a) {
   return 0;
 }
 
+template <typename T>
+std::vector<T> readBin(const std::string& path) {
+  std::ifstream f(path, std::ios::binary | std::ios::ate);
+  if (!f) throw std::runtime_error("cannot read " + path);
+  const std::streamsize bytes = f.tellg();
+  f.seekg(0);
+  std::vector<T> v(static_cast<size_t>(bytes) / sizeof(T));
+  f.read(reinterpret_cast<char*>(v.data()), bytes);
+  return v;
+}
+
+int runCsr(const Args& a) {
+  const std::string in = get(a, "in", "");
+  const std::string out = get(a, "out", "");
+  std::vector<uint64_t> ro = readBin<uint64_t>(in + "/offsets.bin");
+  std::vector<uint64_t> ci = readBin<uint64_t>(in + "/columns.bin");
+  std::vector<double> va = readBin<double>(in + "/values.bin");
+  const std::vector<double> rhs = readBin<double>(in + "/rhs.bin");
+  const std::vector<double> x0 = readBin<double>(in + "/x0.bin");
+  const Index n = ro.size() - 1;
+  std::vector<Index> off(ro.begin(), ro.end()), col(ci.begin(), ci.end());
+  algebra::Vector b(n), x(n);
+  for (Index i = 0; i < n; ++i) {
+    b[i] = rhs[i];
+    x[i] = x0[i];
+  }
+  const algebra::LinearSystem system(
+      algebra::SparseMatrix(n, n, std::move(va), std::move(col), std::move(off)), b);
+  algebra::LinearSolverSettings s;
+  s.absoluteTolerance = getd(a, "atol", 1e-12);
+  s.relativeTolerance = getd(a, "rtol", 1e-10);
+  s.maxIterations = static_cast<Index>(geti(a, "maxit", 1000));
+  std::shared_ptr<algebra::Preconditioner> pre;
+  if (get(a, "pre", "none") == "jacobi") pre = std::make_shared<algebra::JacobiPreconditioner>();
+  std::unique_ptr<algebra::LinearSolver> solver;
+  if (get(a, "solver", "bicgstab") == "cg")
+    solver = std::make_unique<algebra::CG>(s, pre);
+  else
+    solver = std::make_unique<algebra::BiCGSTAB>(s, pre);
+  const algebra::SolverResult r = solver->solve(system, x);
+  const algebra::Vector ax = system.matrix().multiply(r.solution);
+  double rr = 0.0;
+  for (Index i = 0; i < n; ++i) rr += (b[i] - ax[i]) * (b[i] - ax[i]);
+  std::printf(
+      "{\"status\": \"%s\", \"iterations\": %zu, \"restarts\": %zu, \"initial_residual\": %.17g, "
+      "\"final_residual\": %.17g, \"true_residual\": %.17g, \"history\": %zu}\n",
+      solverStatusText(r.status), static_cast<size_t>(r.iterations),
+      static_cast<size_t>(r.restarts), r.initialResidual, r.finalResidual, std::sqrt(rr),
+      r.residualHistory.size());
+  if (!out.empty()) {
+    writeBin(out + "/x.bin", r.solution.data(), n);
+    writeBin(out + "/hist.bin", r.residualHistory);
+  }
+  return 0;
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
   if (argc < 2) {
-    std::fprintf(stderr, "usage: ref_driver poisson|simple key=value ...\n");
+    std::fprintf(stderr, "usage: ref_driver poisson|simple|csr key=value ...\n");
     return 2;
   }
   Args a;
@@ -410,6 +474,7 @@ int main(int argc, char** argv) {
   try {
     if (cmd == "poisson") return runPoisson(a);
     if (cmd == "simple") return runSimple(a);
+    if (cmd == "csr") return runCsr(a);
   } catch (const std::exception& e) {
     std::fprintf(stderr, "ref_driver: %s\n", e.what());
     return 1;
