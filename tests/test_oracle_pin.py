@@ -69,7 +69,7 @@ def test_poisson_matches_golden(name):
 # (the 129^2 configuration-1 run takes the CPU restatement about an hour: it
 # pins the GPU path only, tests/test_simple_gpu.py)
 @pytest.mark.parametrize("name", [n for n in _fixtures("")
-                                  if not n.startswith(("poisson", "results_"))
+                                  if not n.startswith(("poisson", "results_", "csr_", "fullsize_"))
                                   and "_129_" not in n])
 def test_simple_matches_golden(name):
     g = np.load(os.path.join(GOLDEN, name + ".npz"))
