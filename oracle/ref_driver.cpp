@@ -22,7 +22,7 @@
 //          [scheme=upwind|central|lud|quick] [flux=auto|linear|rhiechow]
 //          [mabs=1e-10] [mrel=1e-8] [mmax=500]
 //          [psolver=cg|bicgstab] [ppre=jacobi|none] [pabs=0] [prel=1e-8] [pmax=5000]
-//          [out=DIR]
+//          [mbackend=cpu|gpu] [pbackend=cpu|gpu] [out=DIR]
 //       the reference SIMPLE::solve (SIMPLE.cpp:148) on a uniform Cartesian
 //       lid-driven cavity (Wall x3 + MovingWall{lid,0}) or channel (Inlet
 //       {inlet,0} left, Outlet right, Walls; pressure FixedValue(0) at the
@@ -60,6 +60,7 @@
 #include "cfd/fields/ScalarField.hpp"
 #include "cfd/fields/SurfaceField.hpp"
 #include "cfd/fields/VectorField.hpp"
+#include "cfd/gpu/GPUExecutionStats.hpp"
 #include "cfd/mesh/MeshGeometry.hpp"
 #include "cfd/physics/FluidProperties.hpp"
 #include "cfd/pressure_velocity/PressureCorrectionEquation.hpp"
@@ -298,6 +299,8 @@ algebra::LinearSolverSettings linSettings(const Args& a, const std::string& pref
                                                    : algebra::LinearSolverType::BiCGSTAB;
   s.preconditioner = get(a, prefix + "pre", pre) == "jacobi" ? algebra::PreconditionerType::Jacobi
                                                              : algebra::PreconditionerType::None;
+  s.backend = get(a, prefix + "backend", "cpu") == "gpu" ? algebra::LinearSolverBackend::GPU
+                                                         : algebra::LinearSolverBackend::CPU;
   return s;
 }
 
@@ -363,14 +366,19 @@ int runSimple(const Args& a) {
       "\"global_imbalance\": %.17g, \"momentum_linear_iterations\": %zu, "
       "\"pressure_linear_iterations\": %zu, \"seconds\": %.6f, \"pressure_solve_seconds\": %.6f, "
       "\"momentum_assembly_seconds\": %.6f, \"momentum_solve_seconds\": %.6f, "
-      "\"pressure_assembly_seconds\": %.6f, \"cells\": %zu, \"faces\": %zu}\n",
+      "\"pressure_assembly_seconds\": %.6f, \"cells\": %zu, \"faces\": %zu, "
+      "\"gpu_simple_loop\": %s, \"gpu_fallback_reason\": \"%s\", \"gpu_linear_solves\": %llu, "
+      "\"gpu_backend_fallbacks\": %llu}\n",
       simpleStatusName(r.status), static_cast<size_t>(r.iterations), r.finalUResidual,
       r.finalVResidual, r.finalWResidual, r.finalPressureResidual, r.finalContinuityResidual,
       r.globalMassImbalance, static_cast<size_t>(r.momentumLinearIterations),
       static_cast<size_t>(r.pressureLinearIterations), seconds, r.stageSeconds.pressureSolve,
       r.stageSeconds.momentumAssembly, r.stageSeconds.momentumSolve,
       r.stageSeconds.pressureAssembly, static_cast<size_t>(cells),
-      static_cast<size_t>(m.numberOfFaces()));
+      static_cast<size_t>(m.numberOfFaces()), r.residentSimpleLoop ? "true" : "false",
+      r.gpuDiscretizationFallbackReason.c_str(),
+      static_cast<unsigned long long>(gpu::gpuExecutionStats().gpuLinearSolves),
+      static_cast<unsigned long long>(gpu::gpuExecutionStats().gpuBackendFallbacks));
   if (!out.empty()) {
     std::vector<double> u(cells), v(cells), w(cells), p(cells);
     for (Index i = 0; i < cells; ++i) {

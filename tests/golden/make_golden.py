@@ -29,6 +29,9 @@ SIMPLE = {
                              "pmax=2000 outer=6000", ["u", "v", "p", "flux"]),
     # configuration 1 itself: the 129x129 Re-100 cavity, Jacobi-CG p', to convergence
     "cavity2d_129_config1": ("dim=2 nx=129 ny=129 outer=20000", ["u", "v", "p", "flux"]),
+    # config-1 settings on a 33x33 cavity, to convergence (the C++ drop-in's
+    # linear-solver plugin runs it with the reference's own SIMPLE loop)
+    "cavity2d_33_jacobicg": ("dim=2 nx=33 ny=33 outer=20000", ["u", "v", "p", "flux"]),
     # config-1 settings (Jacobi-CG p') on a small grid, to convergence
     "cavity2d_16_jacobicg": ("dim=2 nx=16 ny=16 outer=6000", ["u", "v", "p", "flux"]),
     "cavity2d_16_lud": ("dim=2 nx=16 ny=16 scheme=lud outer=200", ["u", "v", "p", "flux"]),

@@ -42,3 +42,22 @@ def test_synth_rhs_matches_oracle_bitwise():
     from oracle import oracle as O
     for dim, n in ((2, 48), (3, 12)):
         assert (cfdb.synth_rhs(dim, n) == O.synth_rhs(dim, n)).all()
+
+
+def test_shim_implements_the_reference_gpu_seam():
+    """The drop-in's static library defines the reference's link-time GPU
+    seam (include/cfd/gpu/GPUBackend.hpp:15, GpuLinearSolver.hpp:48-54,
+    GPUExecutionStats.hpp:146-150) and the SIMPLE class; the driver linked
+    with it does not carry the reference's CPU stubs of that seam."""
+    import subprocess
+    lib = os.path.join(ROOT, "cfdapp_b200", "shim", "_out", "libcfdb_shim.a")
+    drv = os.path.join(ROOT, "oracle", "_ref", "ref_driver_cfdb")
+    if not (os.path.exists(lib) and os.path.exists(drv)):
+        pytest.skip("the drop-in is built only where the reference checkout is present")
+    out = subprocess.run(["nm", "-C", "--defined-only", lib], capture_output=True, text=True,
+                         check=True).stdout
+    for sym in ("cfd::gpu::cudaAvailable()", "cfd::gpu::makeGpuCG(", "cfd::gpu::makeGpuBiCGSTAB(",
+                "cfd::gpu::gpuExecutionStats()", "cfd::pressure_velocity::SIMPLE::solve("):
+        assert sym in out, sym
+    dyn = subprocess.run(["readelf", "-d", drv], capture_output=True, text=True, check=True).stdout
+    assert "libcfdb.so" in dyn
