@@ -54,6 +54,18 @@ def parse():
                          "case's convergence test, instead of timing a few")
     ap.add_argument("--history-out", default=None)
     ap.add_argument("--cases", type=int, default=64)
+    ap.add_argument("--no-config1", action="store_true",
+                    help="skip the 129^2 cavity (configuration 1) run to convergence on the GPU")
+    ap.add_argument("--profile-solve", action="store_true",
+                    help="one p' solve of the isolated --dim/--n system and nothing else, for "
+                         "profilers (with CFDB_LEARNED_LAUNCH=stream the learned solve launches "
+                         "its kernels one by one instead of as one graph)")
+    ap.add_argument("--dim", type=int, default=2)
+    ap.add_argument("--n", type=int, default=2048)
+    ap.add_argument("--preconditioner", default="learned_mg",
+                    choices=["learned_mg", "jacobi", "none"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32_refined"])
+    ap.add_argument("--max-iterations", type=int, default=100000)
     return ap.parse_args()
 
 
@@ -156,104 +168,156 @@ def measured_peaks():
 
 
 # ------------------------------------------------------------------ CPU baseline
-def cpu_baseline(grids, iterations_by_grid, sample_iterations=10, repeat=1):
-    """The reference's CG + Jacobi (oracle/_ref: the reference's own
-    CG.cpp/Preconditioner.cpp/SparseMatrix.cpp, OpenMP over all host cores)
-    timed for a bounded sample of `sample_iterations` CG iterations on each
-    grid's system, scaled to the full solve by the iteration count the full
-    solve needs (the same Jacobi-PCG iteration count).  Falls back to the CPU
-    port (oracle/cfdb_oracle.c, one thread) when the reference build is absent.
-    Returns per-repeat step times (ms) and the descriptive dict."""
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+# DRAM bytes per launch of the timed kernels, from ncu captures whose
+# summaries are in profiles/ (learned_fcg_*_launches.md: every kernel of one
+# learned-FCG solve graph summed, mean of the 2048^2 and 256^3 solves;
+# batched_simple_64cases_iteration.md: the batched p' team kernel).
+NCU_TRAFFIC = {"learned_fcg_bytes_per_launch": 77925000000.0,
+               "batched_pprime_dram_bytes_per_launch": 521465025024.0}
+
+
+def reference_full_runs():
+    """The reference's own full CG + Jacobi solves of the two systems, run to
+    rel-res 1e-8 from its sources on every core of the build host
+    (tests/golden/make_fullsize_golden.py): iterations and wall time."""
+    out = {}
+    for dim, n in GRIDS:
+        path = os.path.join(GOLDEN, f"fullsize_{dim}d{n}.npz")
+        if os.path.exists(path):
+            meta = json.loads(str(np.load(path)["meta"]))
+            out[(dim, n)] = meta
+    return out
+
+
+def reference_timing(dim, n, budgets, threads):
+    """The reference's CG + Jacobi (oracle/_ref: CG.cpp, Preconditioner.cpp,
+    SparseMatrix.cpp with OpenMP) on the isolated system, one solve from
+    x0 = 0 per iteration budget: [(budget, iterations, seconds), ...]."""
+    from oracle import oracle as O
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+    out = subprocess.run([O.REF_DRIVER, "poisson", f"dim={dim}", f"n={n}", "direct=1",
+                          "maxits=" + ",".join(str(b) for b in budgets)],
+                         capture_output=True, text=True, env=env, check=True)
+    return json.loads(out.stdout)["maxit_seconds"]
+
+
+def estimate_full_solve(samples, iterations):
+    """Setup plus first iteration (the 1-iteration budget) and the
+    per-iteration time (difference of the two budgets) give the full solve of
+    `iterations` iterations."""
+    (b1, _, t1), (b2, _, t2) = samples[0], samples[-1]
+    per_it = (t2 - t1) / (b2 - b1)
+    return t1 + (iterations - 1) * per_it, per_it, t1
+
+
+def cpu_baseline(grids, fallback_iterations, sample=10):
+    """The reference's own CPU path on the box's host cores: per grid, the
+    setup and per-iteration time of its CG + Jacobi (all cores, and 1 core)
+    from budgets of 1 and `sample` iterations, times the iteration count of
+    the reference's own full solve of that system.  Falls back to the CPU
+    port (oracle/cfdb_oracle.c, one thread) when the reference build is
+    absent."""
     from oracle import oracle as O
     cores = os.cpu_count() or 1
-    kind = "reference" if O.ref_driver_available() else "port"
-    steps = [0.0] * repeat
-    samples = []
-    for dim, n in grids:
-        full_it = iterations_by_grid[(dim, n)]
-        if kind == "reference":
-            env = dict(os.environ, OMP_NUM_THREADS=str(cores))
-            out = subprocess.run([O.REF_DRIVER, "poisson", f"dim={dim}", f"n={n}",
-                                  f"maxit={sample_iterations}", "direct=1", f"repeat={repeat}"],
-                                 capture_output=True, text=True, env=env, check=True)
-            secs = json.loads(out.stdout)["repeat_seconds"]
-        else:
-            cores = 1
+    full = reference_full_runs()
+    if not O.ref_driver_available():
+        total, parts = 0.0, []
+        for dim, n in grids:
             case, fc, diag, off, b = O.isolated_pprime(dim, n)
-            secs = []
-            for _ in range(repeat):
-                t0 = time.perf_counter()
-                O.stencil_solve(case, diag, off, b, max_iterations=sample_iterations,
-                                history=False)
-                secs.append(time.perf_counter() - t0)
-        for q in range(repeat):
-            steps[q] += secs[q] / sample_iterations * full_it * 1e3
-        samples.append(f"{dim}D {n}: {sample_iterations} CG iterations timed, scaled by "
-                       f"{full_it}/{sample_iterations} to the full solve")
-    info = {"value": statistics.mean(steps), "unit": "ms", "cores": cores, "kind": kind,
-            "sample": "; ".join(samples)}
-    return steps, info
+            t0 = time.perf_counter()
+            O.stencil_solve(case, diag, off, b, max_iterations=sample, history=False)
+            per = (time.perf_counter() - t0) / sample
+            its = full.get((dim, n), {}).get("iterations", fallback_iterations[(dim, n)])
+            total += per * its * 1e3
+            parts.append(f"{dim}D {n}: {sample} iterations of the CPU port x {its}")
+        return {"value": total, "unit": "ms", "cores": 1, "kind": "port",
+                "sample": "; ".join(parts)}
+    total = total1 = 0.0
+    parts, detail = [], {}
+    for dim, n in grids:
+        ref = full.get((dim, n))
+        its = ref["iterations"] if ref else fallback_iterations[(dim, n)]
+        src = "the reference's own full solve" if ref else "the device FP64 PCG (no reference run)"
+        est, per_it, setup = estimate_full_solve(reference_timing(dim, n, (1, sample), cores), its)
+        est1, per_it1, _ = estimate_full_solve(reference_timing(dim, n, (1, 2), 1), its)
+        total += est * 1e3
+        total1 += est1 * 1e3
+        detail[f"{dim}D {n}"] = {
+            "iterations": its, "iterations_from": src, "setup_s": setup,
+            "per_iteration_s": per_it, "per_iteration_s_1core": per_it1,
+            "full_solve_estimate_s": est, "full_solve_estimate_s_1core": est1,
+            "full_solve_measured_s_build_host": ref["seconds"] if ref else None,
+            "full_solve_measured_threads_build_host": ref["threads"] if ref else None}
+        parts.append(f"{dim}D {n}: CG + Jacobi budgets of 1 and {sample} iterations timed "
+                     f"({cores} cores; 1 and 2 on 1 core), setup + {its} x per-iteration time")
+    return {"value": total, "unit": "ms", "cores": cores, "kind": "reference",
+            "sample": "; ".join(parts), "value_1core": total1, "grids": detail}
 
 
 # ------------------------------------------------------------------ reference arm
 def run_reference(a, grids):
+    """bench.py --impl reference: the reference's own CPU CG + Jacobi on the
+    same two systems, all host cores.  A full solve takes the reference
+    minutes to an hour per grid, so each step is a bounded sample: per grid a
+    solve with a 1-iteration and one with a 6-iteration budget (the
+    difference is the per-iteration time), giving setup + N x per-iteration
+    with N the iteration count of the reference's own full solve of the
+    system (tests/golden/fullsize_*.npz)."""
     rank, world, _ = dist_info()
     if rank != 0:
         return 0
-    # iteration counts of the full solves come from the oracle's own CG on a
-    # bounded problem? No: the reference CG's full solve is infeasible inside a
-    # few minutes at these sizes, so the iteration count is that of the FP64
-    # Jacobi-PCG solve (identical algorithm) recorded by the device arm when
-    # available, else estimated from the reference's own count on the grid
-    # halved (CG iterations scale ~ linearly with n).
     from oracle import oracle as O
+    if not O.ref_driver_available():
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "the reference build (oracle/_ref) is missing"}))
+        return 0
+    cores = os.cpu_count() or 1
+    full = reference_full_runs()
     its = {}
     for dim, n in grids:
-        its[(dim, n)] = _estimate_iterations(O, dim, n)
+        if (dim, n) in full:
+            its[(dim, n)] = full[(dim, n)]["iterations"]
+        else:  # a grid without a stored reference run: the reference's own
+            # count on the grid halved, scaled (CG iterations grow ~ n here)
+            case, fc, diag, off, b = O.isolated_pprime(dim, n // 2)
+            its[(dim, n)] = 2 * O.stencil_solve(case, diag, off, b, history=False).iterations
     t0 = time.perf_counter()
-    steps, base = cpu_baseline(grids, its, sample_iterations=5, repeat=a.warmup + a.steps)
+    steps = []
+    per_grid = {}
+    for q in range(a.warmup + a.steps):
+        tot = 0.0
+        for dim, n in grids:
+            est, per_it, setup = estimate_full_solve(reference_timing(dim, n, (1, 6), cores),
+                                                     its[(dim, n)])
+            tot += est * 1e3
+            per_grid[f"{dim}D {n}"] = {"setup_s": setup, "per_iteration_s": per_it,
+                                       "iterations": its[(dim, n)], "estimate_s": est}
+        steps.append(tot)
     value = statistics.mean(steps[a.warmup:])
-    base["value"] = value
+    sample = "; ".join(f"{k}: budgets of 1 and 6 CG iterations timed per step, setup + "
+                       f"{v['iterations']} (the reference's own full-solve count) x per-iteration"
+                       for k, v in per_grid.items())
     line = {"metric": METRIC, "value": value, "unit": "ms", "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": value, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "impl": "reference",
             "config": {"workload": "isolated p' solve: 5-point 2048^2 + 7-point 256^3, "
                                    "Neumann + pinned cell, seeded 32-sinusoid RHS, x0=0, "
-                                   "rel-res 1e-8",
+                                   "rel-res 1e-8 (FP64-verified)",
                        "grids": [f"{d}D {n}" for d, n in grids]},
-            "cpu_baseline": base,
+            "cpu_baseline": {"value": value, "unit": "ms", "cores": cores, "kind": "reference",
+                             "sample": sample},
             "e2e": {"value": value, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "iterations_used": {f"{d}D {n}": v for (d, n), v in its.items()},
+            "grids": per_grid,
+            "full_solves_measured_build_host": {
+                f"{d}D {n}": {"iterations": m["iterations"], "seconds": m["seconds"],
+                              "threads": m["threads"], "status": m["status"]}
+                for (d, n), m in full.items()},
             "wall_s": time.perf_counter() - t0}
     print(json.dumps(line), flush=True)
     return 0
-
-
-def _estimate_iterations(O, dim, n):
-    """Jacobi-PCG iterations of the full system: from the persisted device
-    measurement when present, else the oracle's count on a reduced grid scaled
-    linearly in n (CG iterations grow ~ n for this operator)."""
-    path = os.path.join(ROOT, "profiles", "iterations.json")
-    try:
-        with open(path) as f:
-            d = json.load(f)
-        return int(d[f"{dim}D {n}"])
-    except (OSError, KeyError, ValueError):
-        pass
-    m = min(n, 256 if dim == 2 else 32)
-    case, fc, diag, off, b = O.isolated_pprime(dim, m)
-    r = O.stencil_solve(case, diag, off, b, history=False)
-    return int(r.iterations * n / m)
-
-
-def _traffic(key):
-    """DRAM bytes per launch recorded from an ncu capture (profiles/traffic.json)."""
-    try:
-        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
-            return json.load(f).get(key)
-    except (OSError, ValueError):
-        return None
 
 
 # ------------------------------------------------------------------ batched SIMPLE
@@ -422,7 +486,7 @@ def run_batched(a):
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak if achieved else None,
                          "peak_source": f"{peak_kind} hbm_gbs",
-                         "traffic": _traffic("batched_pprime_dram_bytes_per_launch")},
+                         "traffic": NCU_TRAFFIC["batched_pprime_dram_bytes_per_launch"]},
             "e2e": {"value": e2e_work / (e2e_ms * 1e-3), "unit": "cell outer-iterations/s",
                     "h2d_bytes_per_step": h2d // max(a.steps, 1),
                     "d2h_bytes_per_step": d2h // max(a.steps, 1)},
@@ -532,9 +596,119 @@ def run_cavity3d(a):
     return 0
 
 
+# ------------------------------------------------------------------ profiling and setup costs
+def run_profile_solve(a):
+    """One solve of the isolated p' system (seeded RHS, x0 = 0, rel-res
+    1e-8) with the chosen preconditioner and precision, for profilers."""
+    from cfdapp_b200 import cfdb
+    ctx = cfdb.Context(0)
+    b = cfdb.synth_rhs(a.dim, a.n, SEED)
+    op = cfdb.POperator(ctx, a.dim, [a.n] * a.dim)
+    bd = ctx.to_device(b)
+    xd = ctx.alloc(b.nbytes)
+    ctx.memset(xd, 0, b.nbytes)
+    s = cfdb.LinearSolverSettings(absolute_tolerance=0.0, relative_tolerance=1e-8,
+                                  max_iterations=a.max_iterations, preconditioner=a.preconditioner,
+                                  precision=a.precision)
+    r = op.solve_device(bd, xd, s)
+    print(f"{a.dim}D {a.n}: {r.status} in {r.iterations} iterations, {r.device_ms:.3f} ms, "
+          f"true rel-res {r.true_residual / r.initial_residual:.3e}")
+    ctx.free(bd)
+    ctx.free(xd)
+    op.close()
+    ctx.close()
+    return 0
+
+
+def unit_faces(dim, n):
+    """Face coefficients (global face order) of an n^dim grid with D = 1 on
+    every internal face and 0 (Neumann) on the boundary."""
+    shape = [n] * dim
+    out = []
+    for a in range(dim):
+        ext = list(shape)
+        ext[a] += 1
+        f = np.ones(ext[::-1])  # z, y, x order: x fastest
+        idx = [slice(None)] * dim
+        idx[dim - 1 - a] = 0
+        f[tuple(idx)] = 0.0
+        idx[dim - 1 - a] = n
+        f[tuple(idx)] = 0.0
+        out.append(f.reshape(-1))
+    return np.concatenate(out)
+
+
+def learned_setup_costs(ctx, settings, grids):
+    """What the warm headline leaves out: the first learned solve on a new
+    operator (hierarchy build, allocations and capture of the solve graph)
+    and a solve right after new coefficient values (the hierarchy refresh
+    every SIMPLE p' solve pays), next to a warm solve of the same operator;
+    host wall time around each call with the device synchronised, operators
+    with unit face coefficients."""
+    from cfdapp_b200 import cfdb
+    out = {}
+    for dim, n in grids:
+        b = cfdb.synth_rhs(dim, n, SEED)
+        faces = unit_faces(dim, n)
+        op = cfdb.POperator(ctx, dim, [n] * dim, face_coeff=faces)
+        bd = ctx.to_device(b)
+        xd = ctx.alloc(b.nbytes)
+
+        def timed():
+            ctx.memset(xd, 0, b.nbytes)
+            ctx.synchronize()
+            t0 = time.perf_counter()
+            r = op.solve_device(bd, xd, settings)
+            ctx.synchronize()
+            return (time.perf_counter() - t0) * 1e3, r
+
+        cold, _ = timed()
+        warm, rw = timed()
+        t0 = time.perf_counter()
+        op.update_faces(faces)
+        upd = (time.perf_counter() - t0) * 1e3
+        refreshed, rr = timed()
+        out[f"{dim}D {n}"] = {"cold_solve_wall_ms": cold, "warm_solve_wall_ms": warm,
+                              "update_faces_wall_ms": upd, "refreshed_solve_wall_ms": refreshed,
+                              "warm_solve_device_ms": rw.device_ms,
+                              "refreshed_solve_device_ms": rr.device_ms,
+                              "iterations": rw.iterations}
+        ctx.free(bd)
+        ctx.free(xd)
+        op.close()
+    return out
+
+
+def config1_on_gpu(ctx):
+    """Configuration 1 (the 129^2 Re-100 cavity, upwind, linear flux,
+    relaxation 0.7/0.3, tolerances 1e-6) from rest to convergence with the
+    learned p' solve to 1e-8, next to the reference's own single-threaded
+    CPU run of the same case (tests/golden/cavity2d_129_config1.npz)."""
+    from cfdapp_b200 import cfdb
+    s = batched_settings()
+    s.pressure_solver.preconditioner = "learned_mg"
+    sim = cfdb.Simple(ctx, cfdb.SimpleCase.cavity(2, 129, mu=0.01), s)
+    sim.set_state(None, None, None, None)
+    t0 = time.perf_counter()
+    r = sim.iterate(20000)
+    wall = time.perf_counter() - t0
+    sim.close()
+    out = {"status": r.status, "outer_iterations": r.iterations, "device_s": r.device_ms * 1e-3,
+           "wall_s": wall, "pprime_s": r.pressure_solve_ms * 1e-3}
+    path = os.path.join(GOLDEN, "cavity2d_129_config1.npz")
+    if os.path.exists(path):
+        m = json.loads(str(np.load(path)["meta"]))
+        out["reference_cpu"] = {"status": m["status"], "outer_iterations": m["iterations"],
+                                "seconds": m["seconds"], "threads": 1,
+                                "where": "the build host (not the GPU box)"}
+    return out
+
+
 # ------------------------------------------------------------------ device arm
 def main():
     a = parse()
+    if a.profile_solve:
+        return run_profile_solve(a)
     if a.workload == "batched":
         return run_batched(a)
     if a.workload == "cavity3d":
@@ -659,13 +833,7 @@ def main():
     kbytes = sum(r.krylov_bytes for rs in per_grid.values() for r in rs)
     klaunch = sum(r.krylov_launches for rs in per_grid.values() for r in rs)
     achieved = (kbytes / klaunch) / ((kms / klaunch) * 1e-3) / 1e9 if kms > 0 else None
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tpath):
-        try:
-            traffic = json.load(open(tpath)).get("learned_fcg_bytes_per_launch")
-        except ValueError:
-            traffic = None
+    traffic = NCU_TRAFFIC["learned_fcg_bytes_per_launch"]
 
     grid_detail = {}
     for (dim, n), rs in per_grid.items():
@@ -683,9 +851,12 @@ def main():
             "fp64_pcg_gbs": f64r.krylov_bytes / (f64r.krylov_ms * 1e-3) / 1e9,
         }
     its = {f"{d}D {n}": fp64[(d, n)][1].iterations for d, n in grids}
-    base = None
+    setup = learned_setup_costs(ctx, smg, grids)
+    base = config1 = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
-        _, base = cpu_baseline(grids, {(d, n): fp64[(d, n)][1].iterations for d, n in grids})
+        base = cpu_baseline(grids, {(d, n): fp64[(d, n)][1].iterations for d, n in grids})
+    if rank == 0 and world == 1 and not a.no_config1:
+        config1 = config1_on_gpu(ctx)
     if rank == 0:
         line = {
             "metric": METRIC, "value": ms_step, "unit": "ms", "n_gpus": world, "steps": a.steps,
@@ -715,6 +886,8 @@ def main():
             "wall_s": wall,
             "cpu_baseline": base,
             "iterations_fp64": its,
+            "learned_setup": setup,
+            "config1": config1,
         }
         print(json.dumps(line), flush=True)
     for s in systems:

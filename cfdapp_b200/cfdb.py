@@ -315,6 +315,16 @@ class POperator:
         self._h = h
         self.cells = int(ctx.lib.cfdb_poperator_cells(h))
 
+    def update_faces(self, face_coeff: np.ndarray):
+        """New face coefficients for an operator made from face coefficients
+        (cfdb_poperator_update_faces): the device arrays, and a learned
+        solve's hierarchy and graph, are kept; their values are refreshed."""
+        fc = np.ascontiguousarray(face_coeff, dtype=np.float64)
+        L = self.ctx.lib
+        L.cfdb_poperator_update_faces.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_double)]
+        self.ctx.check(L.cfdb_poperator_update_faces(self.ctx.handle, self._h, _dp(fc)),
+                       "cfdb_poperator_update_faces")
+
     def apply_device(self, x_dev: int, y_dev: int):
         self.ctx.check(self.ctx.lib.cfdb_poperator_apply(self.ctx.handle, self._h, C.c_void_p(x_dev),
                                                          C.c_void_p(y_dev)), "cfdb_poperator_apply")

@@ -64,7 +64,8 @@ namespace {
 constexpr int kThreads = 256;
 constexpr unsigned long long kBarrierTimeoutNs = 2000000000ull;  // 2 s per barrier wait
 
-enum { OUT_STATUS = 0, OUT_ITER = 1, OUT_B0 = 2, OUT_FINAL = 3, OUT_PCUR = 4, OUT_TIMEOUT = 5 };
+enum { OUT_STATUS = 0, OUT_ITER = 1, OUT_B0 = 2, OUT_FINAL = 3, OUT_PCUR = 4, OUT_TIMEOUT = 5,
+       OUT_REPLACEMENTS = 6 };
 
 template <typename T>
 OpView<T> view(const cfdb_poperator* op) {
@@ -103,6 +104,15 @@ struct PcgParams {
   double* partials;
   GridSync sync;
   double* out;
+  // mixed precision (T = float): the iterate, right-hand side and residual
+  // replacement live in FP64 (x64, b64, A64); r, p, z are FP32.  The FP32
+  // residual recurrence is replaced by the FP64 b - A x whenever it has
+  // fallen by `delta` since the last replacement, when it reaches the
+  // tolerance, and at the iteration cap.
+  OpView<double> A64;
+  const double* b64;
+  double* x64;
+  double delta;
 };
 
 __device__ __forceinline__ bool finite(double v) { return isfinite(v); }
@@ -440,7 +450,7 @@ bool getenv_flag(const char* name) {
   return v && v[0] && v[0] != '0';
 }
 
-template <typename T, class S>
+template <typename T, class S, bool MIXED = false>
 cfdb_status launch_pcg_tma(cfdb_context* ctx, PcgParams<T>& P) {
   TmaParams<T> TP{};
   const CUtensorMapDataType dt = sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64
@@ -459,10 +469,12 @@ cfdb_status launch_pcg_tma(cfdb_context* ctx, PcgParams<T>& P) {
   if (!encode_tensor_map(&TP.maps.z_halo, dt, es, rank, P.z, dims, halo) ||
       !encode_tensor_map(&TP.maps.p0_halo, dt, es, rank, P.p0, dims, halo) ||
       !encode_tensor_map(&TP.maps.p1_halo, dt, es, rank, P.p1, dims, halo) ||
-      !encode_tensor_map(&TP.maps.x_int, dt, es, rank, P.x, dims, intr) ||
+      // MIXED keeps x in FP64 and updates it with plain loads: its map is
+      // never used and points at r only to stay well formed
+      !encode_tensor_map(&TP.maps.x_int, dt, es, rank, MIXED ? P.r : P.x, dims, intr) ||
       !encode_tensor_map(&TP.maps.r_int, dt, es, rank, P.r, dims, intr))
     return set_error(ctx, CFDB_ERR_CUDA, "cuTensorMapEncodeTiled rejected a p' tensor map");
-  auto kernel = P.A.fx ? pcg_tma<T, S, true> : pcg_tma<T, S, false>;
+  auto kernel = P.A.fx ? pcg_tma<T, S, true, MIXED> : pcg_tma<T, S, false, MIXED>;
   const size_t smem = sizeof(T) * (size_t)S::STAGE * 2;
   CFDB_CUDA(ctx, cudaFuncSetAttribute((const void*)kernel,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -531,6 +543,56 @@ cfdb_status run_pcg(cfdb_context* ctx, const cfdb_poperator* op, const T* b, T* 
   }
   P.cs = make_split<Tile2D>(op->knx, op->kny, op->knz);
   return launch_pcg<T, Tile2D>(ctx, P);
+}
+
+// The mixed-precision PCG (FP32 r, p, z; FP64 x with FP64 residual
+// replacement) on the TMA kernel; needs rows of a multiple of 16 bytes in
+// FP32 (nx % 4 == 0).
+cfdb_status run_pcg_mixed(cfdb_context* ctx, const cfdb_poperator* op, const double* b64,
+                          double* x64, float* r, float* p0, float* p1, float* z, int x0_zero,
+                          double abs_tol, double rel_tol, int64_t max_it, double delta,
+                          double* hist_dev, int64_t hist_cap) {
+  PcgParams<float> P{};
+  P.A = view<float>(op);
+  P.A64 = view<double>(op);
+  P.invd = op->invd32;
+  P.b = nullptr;
+  P.x = nullptr;
+  P.b64 = b64;
+  P.x64 = x64;
+  P.r = r;
+  P.p0 = p0;
+  P.p1 = p1;
+  P.z = z;
+  P.x0_zero = x0_zero;
+  P.abs_tol = abs_tol;
+  P.rel_tol = rel_tol;
+  P.max_it = max_it;
+  P.delta = delta;
+  P.hist = hist_dev;
+  P.hist_cap = hist_cap;
+  if (is3d(op)) {
+    P.cs = make_split<TmaTile3D<float>>(op->knx, op->kny, op->knz);
+    return launch_pcg_tma<float, TmaTile3D<float>, true>(ctx, P);
+  }
+  P.cs = make_split<TmaTile2D<float>>(op->knx, op->kny, op->knz);
+  return launch_pcg_tma<float, TmaTile2D<float>, true>(ctx, P);
+}
+
+// Algorithmic bytes of one mixed-precision PCG launch: per iteration the
+// FP32 words of the TMA kernel (sweep A: z, p_old in, p out; sweep B: p, r
+// in, r, z out) and the FP64 iterate read and written; per residual
+// replacement (and the initial residual) x (unless zero), b in FP64 and r, z
+// out in FP32; face coefficients (FP32) read by every sweep.
+double pcg_mixed_bytes(const cfdb_poperator* op, int64_t iterations, int64_t replacements,
+                       bool x0_zero) {
+  const double cells = (double)op->cells;
+  int fw = 0;
+  for (int q = 0; q < 3; ++q) fw += op->f64[q] ? 1 : 0;
+  const double per_it = cells * ((7.0 + 2.0 * fw) * 4.0 + 16.0);
+  const double per_repl = cells * (16.0 + (2.0 + fw) * 4.0);
+  const double init = cells * ((x0_zero ? 8.0 : 16.0) + (2.0 + fw) * 4.0);
+  return init + per_it * (double)iterations + per_repl * (double)replacements;
 }
 
 // Algorithmic bytes of one persistent PCG launch: the initial pass reads b
@@ -660,7 +722,36 @@ cfdb_status solve_fp64(cfdb_context* ctx, cfdb_poperator* op, const cfdb_linear_
   return add_krylov_time(ctx, res);
 }
 
-// FP32 inner sweeps inside FP64 iterative refinement.
+// FP32 Jacobi-PCG with FP64 residual replacement (one Krylov space).
+cfdb_status solve_mixed(cfdb_context* ctx, cfdb_poperator* op, const cfdb_linear_settings* s,
+                        const double* b, double* x, int64_t hist_cap,
+                        cfdb_linear_result* res) {
+  const int64_t n = op->cells;
+  for (int q : {0, 1, 2, 5}) {
+    cfdb_status st = alloc_vec(ctx, &op->w32[q], n);
+    if (st != CFDB_OK) return st;
+  }
+  cfdb_status st = ensure_hist(ctx, op, std::max<int64_t>(hist_cap, 1));
+  if (st != CFDB_OK) return st;
+  const double delta = s->inner_rel_tol > 0.0 ? s->inner_rel_tol : 0.1;
+  st = run_pcg_mixed(ctx, op, b, x, op->w32[0], op->w32[1], op->w32[2], op->w32[5], 0, s->abs_tol,
+                     s->rel_tol, s->max_iterations, delta, op->hist_dev, hist_cap);
+  if (st != CFDB_OK) return st;
+  st = read_scalars(ctx, 8);
+  if (st != CFDB_OK) return st;
+  const double* o = ctx->scalars_host;
+  res->status = (int)o[OUT_STATUS];
+  res->iterations = (int64_t)o[OUT_ITER];
+  res->initial_residual = o[OUT_B0];
+  res->final_residual = o[OUT_FINAL];
+  res->refinements = (int64_t)o[OUT_REPLACEMENTS];
+  res->krylov_bytes += pcg_mixed_bytes(op, res->iterations, res->refinements, false);
+  return add_krylov_time(ctx, res);
+}
+
+// FP32 inner sweeps inside FP64 iterative refinement (each refinement a new
+// FP32 Krylov solve of the correction): for grids whose rows the TMA kernel
+// cannot take in FP32 (nx % 4 != 0).
 cfdb_status solve_refined(cfdb_context* ctx, cfdb_poperator* op, const cfdb_linear_settings* s,
                           const double* b, double* x, int64_t hist_cap, double* hist_host,
                           cfdb_linear_result* res) {
@@ -1118,6 +1209,13 @@ cfdb_status cfdb_poperator_solve_device(cfdb_context* ctx, const cfdb_poperator*
   CFDB_CUDA(ctx, cudaEventRecord(ctx->ev_start, ctx->stream));
   if (s->preconditioner == CFDB_PRECOND_LEARNED_MG) {
     st = solve_learned(ctx, op, s, b_dev, x_dev, history, history_cap, result);
+  } else if (s->precision == CFDB_PRECISION_FP32_REFINED && pcg_uses_tma(op, sizeof(float))) {
+    st = solve_mixed(ctx, op, s, b_dev, x_dev, history_cap, result);
+    if (st == CFDB_OK && history && history_cap > 0) {
+      const int64_t m = std::min<int64_t>(history_cap, result->iterations + 1);
+      CFDB_CUDA(ctx, cudaMemcpyAsync(history, op->hist_dev, sizeof(double) * m,
+                                     cudaMemcpyDeviceToHost, ctx->stream));
+    }
   } else if (s->precision == CFDB_PRECISION_FP32_REFINED) {
     st = solve_refined(ctx, op, s, b_dev, x_dev, history_cap, history, result);
   } else {

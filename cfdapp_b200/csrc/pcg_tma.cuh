@@ -104,8 +104,15 @@ __device__ __forceinline__ Coef<T> face_coef(const OpView<T>& A, int i, int j, i
 
 constexpr int kTmaThreads = 512;
 
-template <typename T, class S, bool FACE>
+// MIXED (T = float only): FP32 r, p, z with the FP64 iterate x64 updated in
+// sweep B and the residual replaced by the FP64 b - A x (one plain sweep)
+// when the FP32 recurrence has fallen by P.delta since the last
+// replacement, when it reaches the tolerance (so convergence is always
+// decided on the FP64 residual) and at the iteration cap.  One Krylov space
+// for the whole solve: p and the recurrences carry on across replacements.
+template <typename T, class S, bool FACE, bool MIXED>
 __global__ void __launch_bounds__(kTmaThreads, 1) pcg_tma(const __grid_constant__ TmaParams<T> TP) {
+  static_assert(!MIXED || sizeof(T) == 4, "the mixed-precision solve keeps r, p, z in FP32");
   extern __shared__ __align__(128) unsigned char smem_tma[];
   T* stage_mem = reinterpret_cast<T*>(smem_tma);
   __shared__ __align__(8) uint64_t bars[2];
@@ -161,9 +168,45 @@ __global__ void __launch_bounds__(kTmaThreads, 1) pcg_tma(const __grid_constant_
     return true;
   };
 
+  // FP64 residual b64 - A64 x64 of the cells of this block, stored in FP32
+  // with z = D^-1 r (MIXED): the initial residual and every replacement
+  auto true_residual = [&](bool x_zero, double (&acc)[2]) {
+    SlabIter cp{blk};
+    Chunk c;
+    while (cp.template next<S::TZ>(cs, A.nz, S::TX, S::TY, B, c)) {
+      const int n = S::TX * S::TY * (c.z1 - c.z0);
+      for (int q = tid; q < n; q += kTmaThreads) {
+        const int i = c.i0 + q % S::TX, j = c.j0 + (q / S::TX) % S::TY, k = c.z0 + q / (S::TX * S::TY);
+        if (i >= A.nx || j >= A.ny) continue;
+        const int64_t idx = idx_of(i, j, k);
+        double rd = P.b64[idx];
+        if (!x_zero) {
+          const Coef<double> c64 = load_coef(P.A64, i, j, k);
+          auto xv = [&](int ii, int jj, int kk) {
+            return (ii >= 0 && ii < A.nx && jj >= 0 && jj < A.ny && kk >= 0 && kk < A.nz)
+                       ? P.x64[idx_of(ii, jj, kk)] : 0.0;
+          };
+          rd = rd - apply_coef(c64, P.x64[idx], xv(i - 1, j, k), xv(i + 1, j, k), xv(i, j - 1, k),
+                               xv(i, j + 1, k), xv(i, j, k - 1), xv(i, j, k + 1));
+        }
+        const T rn = (T)rd;
+        P.r[idx] = rn;
+        T inv;
+        if constexpr (FACE) inv = __ldg(P.invd + idx);
+        else inv = load_coef(A, i, j, k).inv;
+        const T zn = inv * rn;
+        P.z[idx] = zn;
+        acc[0] += rd * rd;
+        acc[1] += (double)rn * (double)zn;
+      }
+    }
+  };
+
   // ---- r0 = b - A x0 (plain loads: once per solve), ||r0||^2, r0.z0
   double acc[2] = {0.0, 0.0};
-  {
+  if constexpr (MIXED) {
+    true_residual(P.x0_zero != 0, acc);
+  } else {
     SlabIter cp{blk};
     Chunk c;
     while (cp.template next<S::TZ>(cs, A.nz, S::TX, S::TY, B, c)) {
@@ -221,6 +264,8 @@ __global__ void __launch_bounds__(kTmaThreads, 1) pcg_tma(const __grid_constant_
   double res_cur = b0;
   double beta = 0.0;
   bool pold_is_p0 = true;
+  double res_replaced = b0;  // MIXED: FP64 residual at the last replacement
+  int64_t replacements = 0;
   for (int64_t it = 1; it <= P.max_it; ++it) {
     const bool first = (it == 1);
     const T tbeta = (T)beta;
@@ -330,15 +375,16 @@ __global__ void __launch_bounds__(kTmaThreads, 1) pcg_tma(const __grid_constant_
     const bool okB = pipeline(
         [&](const Chunk& c, T* base, uint64_t* bar) {
           fence_proxy_async_smem();
-          mbar_arrive_expect_tx(bar, S::BYTES_B);
+          // MIXED updates the FP64 iterate in place with plain loads: no x box
+          mbar_arrive_expect_tx(bar, MIXED ? (uint32_t)(S::HALO + S::INTR) * sizeof(T) : S::BYTES_B);
           const int hx = c.i0 - S::XO, hy = c.j0 - S::OY, hz = c.z0 - 1;
           if constexpr (S::D3) {
             tma_load_3d(base, pnew_map, hx, hy, hz, bar);
-            tma_load_3d(base + S::HALO_P, &TP.maps.x_int, c.i0, c.j0, c.z0, bar);
+            if constexpr (!MIXED) tma_load_3d(base + S::HALO_P, &TP.maps.x_int, c.i0, c.j0, c.z0, bar);
             tma_load_3d(base + S::HALO_P + S::INTR_P, &TP.maps.r_int, c.i0, c.j0, c.z0, bar);
           } else {
             tma_load_2d(base, pnew_map, hx, hz, bar);
-            tma_load_2d(base + S::HALO_P, &TP.maps.x_int, c.i0, c.z0, bar);
+            if constexpr (!MIXED) tma_load_2d(base + S::HALO_P, &TP.maps.x_int, c.i0, c.z0, bar);
             tma_load_2d(base + S::HALO_P + S::INTR_P, &TP.maps.r_int, c.i0, c.z0, bar);
           }
         },
@@ -389,7 +435,8 @@ __global__ void __launch_bounds__(kTmaThreads, 1) pcg_tma(const __grid_constant_
                 ap = fma(dg, v, -off);
                 inv = rcp_rn(dg);
               }
-              P.x[idx] = fma(talpha, v, xb[q]);
+              if constexpr (MIXED) P.x64[idx] = fma(alpha, (double)v, P.x64[idx]);
+              else P.x[idx] = fma(talpha, v, xb[q]);
               const T rn = fma(-talpha, ap, rb[q]);
               P.r[idx] = rn;
               const T zn = inv * rn;
@@ -408,7 +455,27 @@ __global__ void __launch_bounds__(kTmaThreads, 1) pcg_tma(const __grid_constant_
     if (!okB || !grid_sync(P.sync)) return;
     grid_total<2>(part(), 2, B, tot, red);
     ++round;
-    const double res = sqrt(tot[0]);
+    double res = sqrt(tot[0]);
+    if constexpr (MIXED) {
+      // replace the FP32 recurrence by the FP64 residual (grid-uniform decision)
+      if (finite(res) && (converged(res) || res <= P.delta * res_replaced || it == P.max_it)) {
+        if (!grid_sync(P.sync)) return;  // every x64 update of this iteration is visible
+        double acc2[2] = {0.0, 0.0};
+        true_residual(false, acc2);
+        block_sum<2>(acc2, red);
+        if (tid == 0) {
+          part()[2 * blk] = acc2[0];
+          part()[2 * blk + 1] = acc2[1];
+        }
+        if (!grid_sync(P.sync)) return;
+        grid_total<2>(part(), 2, B, tot, red);
+        ++round;
+        res = sqrt(tot[0]);
+        res_replaced = res;
+        ++replacements;
+        if (leader) P.out[OUT_REPLACEMENTS] = (double)replacements;
+      }
+    }
     if (leader && it < P.hist_cap) P.hist[it] = res;
     if (!finite(res)) {
       if (leader) {

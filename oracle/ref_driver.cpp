@@ -7,7 +7,7 @@
 //
 //   poisson dim=2|3 n=N [seed=S] [rtol=1e-8] [maxit=M] [pre=jacobi|none]
 //           [solver=cg|bicgstab] [out=DIR] [dump_matrix=1] [direct=1] [repeat=R]
-//           [check_direct=1]
+//           [check_direct=1] [maxits=a,b,...]
 //       p' system of the reference's assemblePressureCorrection
 //       (PressureCorrectionEquation.cpp:341) with unit response
 //       coefficients, rho = 1, all-FixedGradient(0) pressure patches and
@@ -242,6 +242,36 @@ int runPoisson(const Args& a) {
     for (Index r = 0; same && r <= A.rows(); ++r) same = A.rowOffsetsData()[r] == B.rowOffsetsData()[r];
     std::printf("{\"direct_matches_reference\": %s}\n", same ? "true" : "false");
     return same ? 0 : 1;
+  }
+  // maxits=a,b,... times one solve from x0 = 0 per iteration budget on the
+  // same matrix (the difference of two budgets is the per-iteration cost
+  // without the solve's setup) and reports `maxit_seconds`.
+  const std::string maxits = get(a, "maxits", "");
+  if (!maxits.empty()) {
+    std::string times;
+    size_t pos = 0;
+    while (pos <= maxits.size()) {
+      const size_t comma = maxits.find(',', pos);
+      const std::string tok = maxits.substr(pos, comma == std::string::npos ? std::string::npos
+                                                                            : comma - pos);
+      algebra::LinearSolverSettings sk = s;
+      sk.maxIterations = static_cast<Index>(std::strtoll(tok.c_str(), nullptr, 10));
+      std::unique_ptr<algebra::LinearSolver> sv;
+      if (get(a, "solver", "cg") == "bicgstab")
+        sv = std::make_unique<algebra::BiCGSTAB>(sk, pre);
+      else
+        sv = std::make_unique<algebra::CG>(sk, pre);
+      const auto t0 = std::chrono::steady_clock::now();
+      const algebra::SolverResult rk = sv->solve(system);
+      const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+      times += (times.empty() ? "" : ", ") + std::string("[") + tok + ", " +
+               std::to_string(rk.iterations) + ", " + std::to_string(sec) + "]";
+      if (comma == std::string::npos) break;
+      pos = comma + 1;
+    }
+    std::printf("{\"maxit_seconds\": [%s], \"cells\": %zu, \"threads\": %d}\n", times.c_str(),
+                static_cast<size_t>(cells), ompThreads());
+    return 0;
   }
   // repeat=R times the same solve R times (each from x0 = 0); the summary
   // reports the last one and `repeat_seconds` lists all.

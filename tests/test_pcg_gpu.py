@@ -41,7 +41,10 @@ def test_isolated_fp64_matches_oracle(ctx, dim, n):
     assert res.kernel_launches >= 1
 
 
-@pytest.mark.parametrize("dim,n", [(2, 64), (2, 300), (3, 24)])
+# nx % 4 == 0: FP32 Jacobi-PCG with FP64 iterate and FP64 residual
+# replacement (one Krylov space); nx % 4 != 0 (66, 26): FP32 solves inside
+# FP64 iterative refinement
+@pytest.mark.parametrize("dim,n", [(2, 64), (2, 300), (3, 24), (2, 66), (3, 26)])
 def test_isolated_fp32_refined_reaches_fp64_tolerance(ctx, dim, n):
     from cfdapp_b200.cfdb import POperator
     case, fc, diag, off, b = O.isolated_pprime(dim, n)
@@ -54,6 +57,49 @@ def test_isolated_fp32_refined_reaches_fp64_tolerance(ctx, dim, n):
     # true residual recomputed on the CPU from the returned x
     ax = O.stencil_apply(case, diag, off, res.solution)
     assert np.linalg.norm(b - ax) / np.linalg.norm(b) <= 1.01e-8
+    assert _rel(res.solution, ref.solution) <= 1e-6
+
+
+@pytest.mark.parametrize("dim,n", [(2, 512), (3, 64)])
+def test_mixed_precision_keeps_one_krylov_space(ctx, dim, n):
+    """The FP32 PCG with FP64 residual replacement needs about as many
+    iterations as the FP64 PCG (it keeps its search directions across
+    replacements), reaches the FP64-verified tolerance, and reports its
+    replacements; its residual history ends with the FP64 residual."""
+    from cfdapp_b200.cfdb import POperator
+    case, fc, diag, off, b = O.isolated_pprime(dim, n)
+    op = POperator(ctx, dim, [n] * dim)
+    r64 = op.solve(b, _settings())
+    r32 = op.solve(b, _settings(precision="fp32_refined"))
+    assert r64.status == r32.status == "Converged"
+    assert r32.iterations <= 1.15 * r64.iterations + 10
+    assert r32.refinements >= 3
+    assert r32.true_residual / r32.initial_residual <= 1e-8
+    ax = O.stencil_apply(case, diag, off, r32.solution)
+    assert np.linalg.norm(b - ax) / np.linalg.norm(b) <= 1.01e-8
+    assert r32.residual_history[-1] == pytest.approx(r32.final_residual, rel=1e-12)
+    assert _rel(r32.solution, r64.solution) <= 1e-6
+    # FP32 vectors: fewer bytes per iteration than the FP64 solve
+    assert r32.krylov_bytes / r32.iterations < 0.7 * r64.krylov_bytes / r64.iterations
+
+
+@pytest.mark.parametrize("dim,n", [(2, 48), (3, 16)])
+def test_mixed_precision_on_face_coefficients(ctx, dim, n):
+    """A SIMPLE-like p' system (variable face coefficients) in FP32 with FP64
+    replacement, against the oracle's FP64 CG."""
+    from cfdapp_b200.cfdb import POperator
+    rng = np.random.default_rng(11)
+    case = O.cavity(dim, n)
+    cells = case.cells()
+    du, dv, dw = (rng.uniform(0.5, 2.0, cells) for _ in range(3))
+    flux = rng.normal(size=case.faces()) * 1e-3
+    fc, diag, off, rhs = O.assemble_pprime(case, 1.0, flux, du, dv, dw)
+    ref = O.stencil_solve(case, diag, off, rhs, rel_tol=1e-10)
+    op = POperator(ctx, dim, [n] * dim, face_coeff=fc)
+    res = op.solve(rhs, _settings(precision="fp32_refined"))
+    assert res.status == "Converged"
+    ax = O.stencil_apply(case, diag, off, res.solution)
+    assert np.linalg.norm(rhs - ax) / np.linalg.norm(rhs) <= 1.01e-8
     assert _rel(res.solution, ref.solution) <= 1e-6
 
 
