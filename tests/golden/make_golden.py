@@ -37,6 +37,10 @@ SIMPLE = {
     "cavity2d_16_lud": ("dim=2 nx=16 ny=16 scheme=lud outer=200", ["u", "v", "p", "flux"]),
     "channel2d_32x8_central_rc": ("dim=2 nx=32 ny=8 lx=8 ly=1 flow=channel mu=0.1 scheme=central "
                                   "flux=rhiechow outer=150", ["u", "v", "p", "flux"]),
+    # configuration 5's discretization (linear upwind + Rhie-Chow, Re 1000,
+    # Jacobi-CG p' to 1e-8) on a 32^3 cavity, to convergence
+    "cavity3d_32_lud_rc_re1000": ("dim=3 nx=32 ny=32 nz=32 mu=0.001 scheme=lud flux=rhiechow "
+                                  "outer=5000", ["u", "v", "w", "p", "flux"]),
     "cavity3d_8_quick_rc": ("dim=3 nx=8 ny=8 nz=8 mu=0.001 scheme=quick flux=rhiechow outer=40 "
                             "psolver=bicgstab ppre=none prel=1e-4 pabs=1e-13 mrel=1e-6 mabs=1e-13 "
                             "tolu=1e-7 tolp=1e-7 tolc=1e-7", ["u", "v", "w", "p", "flux"]),

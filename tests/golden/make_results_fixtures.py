@@ -1,6 +1,8 @@
-"""Fixtures of the reference's result-file formats, taken from two of the
-reference's committed example runs (cases/lid_driven_cavity, 20x20,
-cases/lid_driven_cavity_3d, 16^3, and cases/poiseuille_flow, 64x8): the field values and residual history
+"""Fixtures of the reference's result-file formats, taken from its committed
+example runs of uniform Cartesian laminar cases (cases/lid_driven_cavity,
+20x20, _40x40, _80x80; cases/lid_driven_cavity_3d, 16^3;
+cases/lid_driven_cavity_3d_re1000, 32^3; cases/duct_3d, 48x8x8;
+cases/poiseuille_flow, 64x8): the field values and residual history
 parsed back from their fields.csv / residuals.csv (17 significant digits
 round-trip exactly), the final global mass imbalance, the grid, and the
 SHA-256 and size of each committed fields.csv, residuals.csv and
@@ -21,7 +23,12 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CASES = {"results_cavity2d_20": "lid_driven_cavity", "results_cavity3d_16": "lid_driven_cavity_3d",
-         "results_channel2d_64x8": "poiseuille_flow"}
+         "results_channel2d_64x8": "poiseuille_flow",
+         # the reference's other uniform Cartesian laminar examples: field values only
+         "results_cavity2d_40": "lid_driven_cavity_40x40",
+         "results_cavity2d_80": "lid_driven_cavity_80x80",
+         "results_cavity3d_32_re1000": "lid_driven_cavity_3d_re1000",
+         "results_duct3d_48x8x8": "duct_3d"}
 CASE_FILES = ("case.json", "geometry.json", "mesh.json", "physics.json", "boundaries.json",
               "solver.json")
 

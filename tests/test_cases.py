@@ -79,10 +79,14 @@ def test_refuses_what_is_not_on_the_gpu_path(tmp_path, fn, change):
 def _compare(out_dir, fixture, iterations_bar=0.02):
     g = np.load(os.path.join(GOLDEN, fixture + ".npz"))
     rows = open(os.path.join(out_dir, "fields.csv")).read().splitlines()
+    col = {h: i for i, h in enumerate(rows[0].split(","))}
     f = np.array([[float(x) for x in r.split(",")] for r in rows[1:]])
     rel = lambda a, b: np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
-    assert rel(f[:, 3], g["u"]) <= 1e-6 and rel(f[:, 4], g["v"]) <= 1e-6
-    assert rel(f[:, 6], g["p"]) <= 1e-6
+    assert rel(f[:, col["velocity_x"]], g["u"]) <= 1e-6
+    assert rel(f[:, col["velocity_y"]], g["v"]) <= 1e-6
+    if "velocity_z" in col:
+        assert rel(f[:, col["velocity_z"]], g["w"]) <= 1e-6
+    assert rel(f[:, col["pressure"]], g["p"]) <= 1e-6
     res = open(os.path.join(out_dir, "residuals.csv")).read().splitlines()
     assert abs((len(res) - 1) - len(g["hist"])) <= max(2, iterations_bar * len(g["hist"]))
     assert os.path.exists(os.path.join(out_dir, "solution.vtk"))
@@ -90,7 +94,13 @@ def _compare(out_dir, fixture, iterations_bar=0.02):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("name,fixture", [("lid_driven_cavity", "results_cavity2d_20"),
-                                          ("poiseuille_flow", "results_channel2d_64x8")])
+                                          ("poiseuille_flow", "results_channel2d_64x8"),
+                                          ("lid_driven_cavity_40x40", "results_cavity2d_40"),
+                                          ("lid_driven_cavity_80x80", "results_cavity2d_80"),
+                                          ("lid_driven_cavity_3d", "results_cavity3d_16"),
+                                          ("lid_driven_cavity_3d_re1000",
+                                           "results_cavity3d_32_re1000"),
+                                          ("duct_3d", "results_duct3d_48x8x8")])
 def test_gpu_run_lands_on_the_reference_results(ctx, tmp_path, name, fixture):
     c = cases.read_case(os.path.join(CASES, name))
     row = cases.run_case(ctx, c, str(tmp_path))

@@ -27,7 +27,9 @@ def _case(meta):
 
 
 @pytest.mark.parametrize("name", ["results_cavity2d_20", "results_cavity3d_16",
-                                  "results_channel2d_64x8"])
+                                  "results_channel2d_64x8", "results_cavity2d_40",
+                                  "results_cavity2d_80", "results_cavity3d_32_re1000",
+                                  "results_duct3d_48x8x8"])
 def test_writer_reproduces_the_reference_files(tmp_path, name):
     g, meta = _fixture(name)
     d = str(tmp_path / "results")
