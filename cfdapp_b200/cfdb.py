@@ -342,13 +342,21 @@ class POperator:
     def _result(self, r: _LinResult, hist, cap, sol=None) -> SolverResult:
         if self._precond == PRECOND["learned_mg"]:
             m = r.iterations - r.fallback_iterations + 1
+        elif self._precision == 0 or self._mixed_in_one_space():
+            m = r.iterations + 1  # one entry per iteration
         else:
-            m = (r.iterations + 1) if self._precision == 0 else (r.refinements + 1)
+            m = r.refinements + 1  # FP32 solves inside FP64 refinement: one per refinement
         m = min(cap, m)
         return SolverResult(SOLVER_STATUS[r.status], r.iterations, r.initial_residual,
                             r.final_residual, r.true_residual, r.refinements, r.restarts,
                             r.device_ms, r.kernel_launches, r.krylov_ms, r.krylov_bytes,
                             r.krylov_launches, r.fallback_iterations, hist[:m].copy(), sol)
+
+    def _mixed_in_one_space(self) -> bool:
+        """Whether an FP32_REFINED solve of this operator runs the FP32
+        Jacobi-PCG with FP64 residual replacement (rows of a multiple of 16
+        bytes in FP32) rather than FP32 solves inside FP64 refinement."""
+        return self.n[0] % 4 == 0 and not os.environ.get("CFDB_NO_TMA")
 
     def solve(self, b: np.ndarray, settings: LinearSolverSettings, x0: np.ndarray | None = None,
               history_cap: int | None = None) -> SolverResult:

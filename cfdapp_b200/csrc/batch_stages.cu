@@ -154,7 +154,7 @@ __global__ void k_assemble(BatchDev B, int comp) {
 __global__ void k_response(BatchDev B) {
   for_cells(B, [&](const BCase& K, int k, int64_t c) {
     const int64_t o = K.c0;
-    for (int a = 0; a < K.G.dim; ++a) B.dres[a][o + c] = ops::response(K.G, B.mdiag[a][o + c]);
+    for (int a = 0; a < K.G.dim; ++a) B.dres[a][o + c] = ops::response(K.G, B.mdiag[a][o + c], c);
     // the single-case path checks Us[0], Us[1] and Us[dim-1]
     const bool ok = isfinite(B.Us[0][o + c]) && isfinite(B.Us[1][o + c]) &&
                     isfinite(B.Us[K.G.dim - 1][o + c]);

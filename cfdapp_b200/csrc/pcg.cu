@@ -23,6 +23,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "cfdb.h"
@@ -104,14 +105,16 @@ struct PcgParams {
   double* partials;
   GridSync sync;
   double* out;
-  // mixed precision (T = float): the iterate, right-hand side and residual
-  // replacement live in FP64 (x64, b64, A64); r, p, z are FP32.  The FP32
-  // residual recurrence is replaced by the FP64 b - A x whenever it has
-  // fallen by `delta` since the last replacement, when it reaches the
-  // tolerance, and at the iteration cap.
+  // mixed precision (T = float): the iterate, residual and right-hand side
+  // live in FP64 (x64, r64, b64) and the stencil arithmetic uses the FP64
+  // coefficients (A64); p and z are stored in FP32.  The residual is
+  // replaced by the FP64 b - A x whenever it has fallen by `delta` since
+  // the last replacement, when it reaches the tolerance, and at the
+  // iteration cap.
   OpView<double> A64;
   const double* b64;
   double* x64;
+  double* r64;
   double delta;
 };
 
@@ -549,7 +552,7 @@ cfdb_status run_pcg(cfdb_context* ctx, const cfdb_poperator* op, const T* b, T* 
 // replacement) on the TMA kernel; needs rows of a multiple of 16 bytes in
 // FP32 (nx % 4 == 0).
 cfdb_status run_pcg_mixed(cfdb_context* ctx, const cfdb_poperator* op, const double* b64,
-                          double* x64, float* r, float* p0, float* p1, float* z, int x0_zero,
+                          double* x64, double* r64, float* p0, float* p1, float* z, int x0_zero,
                           double abs_tol, double rel_tol, int64_t max_it, double delta,
                           double* hist_dev, int64_t hist_cap) {
   PcgParams<float> P{};
@@ -560,7 +563,8 @@ cfdb_status run_pcg_mixed(cfdb_context* ctx, const cfdb_poperator* op, const dou
   P.x = nullptr;
   P.b64 = b64;
   P.x64 = x64;
-  P.r = r;
+  P.r64 = r64;
+  P.r = z;  // FP32 residual unused: the TMA map that would carry it points at z
   P.p0 = p0;
   P.p1 = p1;
   P.z = z;
@@ -580,18 +584,18 @@ cfdb_status run_pcg_mixed(cfdb_context* ctx, const cfdb_poperator* op, const dou
 }
 
 // Algorithmic bytes of one mixed-precision PCG launch: per iteration the
-// FP32 words of the TMA kernel (sweep A: z, p_old in, p out; sweep B: p, r
-// in, r, z out) and the FP64 iterate read and written; per residual
-// replacement (and the initial residual) x (unless zero), b in FP64 and r, z
-// out in FP32; face coefficients (FP32) read by every sweep.
+// FP32 words (sweep A: z, p_old in, p out; sweep B: p in, z out) and the FP64
+// x and r read and written in sweep B; per residual replacement (and the
+// initial residual) x (unless zero) and b in, r out in FP64 and z out in
+// FP32; FP64 face coefficients read by every sweep.
 double pcg_mixed_bytes(const cfdb_poperator* op, int64_t iterations, int64_t replacements,
                        bool x0_zero) {
   const double cells = (double)op->cells;
   int fw = 0;
   for (int q = 0; q < 3; ++q) fw += op->f64[q] ? 1 : 0;
-  const double per_it = cells * ((7.0 + 2.0 * fw) * 4.0 + 16.0);
-  const double per_repl = cells * (16.0 + (2.0 + fw) * 4.0);
-  const double init = cells * ((x0_zero ? 8.0 : 16.0) + (2.0 + fw) * 4.0);
+  const double per_it = cells * (5.0 * 4.0 + 4.0 * 8.0 + 2.0 * fw * 8.0);
+  const double per_repl = cells * (3.0 * 8.0 + 4.0 + fw * 8.0);
+  const double init = cells * ((x0_zero ? 2.0 : 3.0) * 8.0 + 4.0 + fw * 8.0);
   return init + per_it * (double)iterations + per_repl * (double)replacements;
 }
 
@@ -727,14 +731,16 @@ cfdb_status solve_mixed(cfdb_context* ctx, cfdb_poperator* op, const cfdb_linear
                         const double* b, double* x, int64_t hist_cap,
                         cfdb_linear_result* res) {
   const int64_t n = op->cells;
-  for (int q : {0, 1, 2, 5}) {
+  for (int q : {1, 2, 5}) {
     cfdb_status st = alloc_vec(ctx, &op->w32[q], n);
     if (st != CFDB_OK) return st;
   }
-  cfdb_status st = ensure_hist(ctx, op, std::max<int64_t>(hist_cap, 1));
+  cfdb_status st = alloc_vec(ctx, &op->w64[0], n);
+  if (st != CFDB_OK) return st;
+  st = ensure_hist(ctx, op, std::max<int64_t>(hist_cap, 1));
   if (st != CFDB_OK) return st;
   const double delta = s->inner_rel_tol > 0.0 ? s->inner_rel_tol : 0.1;
-  st = run_pcg_mixed(ctx, op, b, x, op->w32[0], op->w32[1], op->w32[2], op->w32[5], 0, s->abs_tol,
+  st = run_pcg_mixed(ctx, op, b, x, op->w64[0], op->w32[1], op->w32[2], op->w32[5], 0, s->abs_tol,
                      s->rel_tol, s->max_iterations, delta, op->hist_dev, hist_cap);
   if (st != CFDB_OK) return st;
   st = read_scalars(ctx, 8);

@@ -104,21 +104,35 @@ __device__ __forceinline__ Coef<T> face_coef(const OpView<T>& A, int i, int j, i
 
 constexpr int kTmaThreads = 512;
 
-// MIXED (T = float only): FP32 r, p, z with the FP64 iterate x64 updated in
-// sweep B and the residual replaced by the FP64 b - A x (one plain sweep)
-// when the FP32 recurrence has fallen by P.delta since the last
-// replacement, when it reaches the tolerance (so convergence is always
-// decided on the FP64 residual) and at the iteration cap.  One Krylov space
-// for the whole solve: p and the recurrences carry on across replacements.
+// The coefficient view the stencil arithmetic of a sweep uses.
+template <bool MIXED, typename T>
+__device__ __forceinline__ const auto& coef_view(const PcgParams<T>& P) {
+  if constexpr (MIXED) return P.A64;
+  else return P.A;
+}
+
+// MIXED (T = float only): the search direction p and z = D^-1 r are stored in
+// FP32 (the vectors the TMA boxes carry); the iterate x and the residual r
+// stay in FP64 (P.x64, P.r64, plain coalesced loads in sweep B) and every
+// A p is evaluated in FP64 from the FP32-stored p, so the FP64 recurrence
+// r -= alpha A p stays consistent with x += alpha p exactly as in the FP64
+// solve: only the directions are rounded to FP32.  The residual is also
+// replaced by the FP64 b - A x (one plain sweep) when it has fallen by
+// P.delta since the last replacement, when it reaches the tolerance (so
+// convergence is decided on the FP64 residual of the iterate) and at the
+// iteration cap.  One Krylov space for the whole solve.
 template <typename T, class S, bool FACE, bool MIXED>
 __global__ void __launch_bounds__(kTmaThreads, 1) pcg_tma(const __grid_constant__ TmaParams<T> TP) {
-  static_assert(!MIXED || sizeof(T) == 4, "the mixed-precision solve keeps r, p, z in FP32");
+  static_assert(!MIXED || sizeof(T) == 4, "the mixed-precision solve stores p and z in FP32");
+  // coefficients and stencil arithmetic: FP64 in the mixed solve, else T
+  using C = typename std::conditional<MIXED, double, T>::type;
   extern __shared__ __align__(128) unsigned char smem_tma[];
   T* stage_mem = reinterpret_cast<T*>(smem_tma);
   __shared__ __align__(8) uint64_t bars[2];
   __shared__ double red[64];
   const PcgParams<T>& P = TP.P;
   const OpView<T>& A = P.A;
+  const OpView<C>& AC = coef_view<MIXED>(P);
   const int B = gridDim.x, blk = blockIdx.x;
   const int tid = threadIdx.x;
   const bool leader = (blk == 0 && tid == 0);
@@ -168,8 +182,9 @@ __global__ void __launch_bounds__(kTmaThreads, 1) pcg_tma(const __grid_constant_
     return true;
   };
 
-  // FP64 residual b64 - A64 x64 of the cells of this block, stored in FP32
-  // with z = D^-1 r (MIXED): the initial residual and every replacement
+  // FP64 residual b64 - A64 x64 of the cells of this block into r64, with
+  // z = D^-1 r stored in FP32 (MIXED): the initial residual and every
+  // replacement
   auto true_residual = [&](bool x_zero, double (&acc)[2]) {
     SlabIter cp{blk};
     Chunk c;
@@ -179,9 +194,9 @@ __global__ void __launch_bounds__(kTmaThreads, 1) pcg_tma(const __grid_constant_
         const int i = c.i0 + q % S::TX, j = c.j0 + (q / S::TX) % S::TY, k = c.z0 + q / (S::TX * S::TY);
         if (i >= A.nx || j >= A.ny) continue;
         const int64_t idx = idx_of(i, j, k);
+        const Coef<double> c64 = load_coef(P.A64, i, j, k);
         double rd = P.b64[idx];
         if (!x_zero) {
-          const Coef<double> c64 = load_coef(P.A64, i, j, k);
           auto xv = [&](int ii, int jj, int kk) {
             return (ii >= 0 && ii < A.nx && jj >= 0 && jj < A.ny && kk >= 0 && kk < A.nz)
                        ? P.x64[idx_of(ii, jj, kk)] : 0.0;
@@ -189,15 +204,11 @@ __global__ void __launch_bounds__(kTmaThreads, 1) pcg_tma(const __grid_constant_
           rd = rd - apply_coef(c64, P.x64[idx], xv(i - 1, j, k), xv(i + 1, j, k), xv(i, j - 1, k),
                                xv(i, j + 1, k), xv(i, j, k - 1), xv(i, j, k + 1));
         }
-        const T rn = (T)rd;
-        P.r[idx] = rn;
-        T inv;
-        if constexpr (FACE) inv = __ldg(P.invd + idx);
-        else inv = load_coef(A, i, j, k).inv;
-        const T zn = inv * rn;
+        P.r64[idx] = rd;
+        const T zn = (T)(c64.inv * rd);
         P.z[idx] = zn;
         acc[0] += rd * rd;
-        acc[1] += (double)rn * (double)zn;
+        acc[1] += rd * (double)zn;
       }
     }
   };
@@ -312,34 +323,35 @@ __global__ void __launch_bounds__(kTmaThreads, 1) pcg_tma(const __grid_constant_
             if constexpr (FACE) {
               for (int kk = kb; kk < ke; ++kk, e += PL, idx += pstride) {
                 const T hi = pv(e + PL);
-                const Coef<T> cf = face_coef(A, i, j, c.z0 + kk);
-                const T ap = apply_coef(cf, v, pv(e - 1), pv(e + 1), S::D3 ? pv(e - S::HX) : T(0),
-                                        S::D3 ? pv(e + S::HX) : T(0), lo, hi);
+                const Coef<C> cf = face_coef(AC, i, j, c.z0 + kk);
+                const C ap = apply_coef(cf, (C)v, (C)pv(e - 1), (C)pv(e + 1),
+                                        S::D3 ? (C)pv(e - S::HX) : C(0),
+                                        S::D3 ? (C)pv(e + S::HX) : C(0), (C)lo, (C)hi);
                 pnew[idx] = v;
                 pap += (double)v * (double)ap;
                 lo = v;
                 v = hi;
               }
             } else {
-              const ColCoef<T> cc = column_coef(A, i, j);
+              const ColCoef<C> cc = column_coef(AC, i, j);
               for (int kk = kb; kk < ke; ++kk, e += PL, idx += pstride) {
                 const int k = c.z0 + kk;
                 const T hi = pv(e + PL);
-                const T zl_ = __ldg(A.tz + k), zh_ = __ldg(A.tz + k + 1);
-                T ap;
+                const C zl_ = __ldg(AC.tz + k), zh_ = __ldg(AC.tz + k + 1);
+                C ap;
                 if (cc.has_ref && k == cc.ref_k) {
-                  ap = v;
+                  ap = (C)v;
                 } else {
-                  const T dg = (cc.sxy + zl_) + zh_;
-                  T off = cc.cxl * pv(e - 1);
-                  off = fma(cc.cxh, pv(e + 1), off);
+                  const C dg = (cc.sxy + zl_) + zh_;
+                  C off = cc.cxl * (C)pv(e - 1);
+                  off = fma(cc.cxh, (C)pv(e + 1), off);
                   if (S::D3) {
-                    off = fma(cc.cyl, pv(e - S::HX), off);
-                    off = fma(cc.cyh, pv(e + S::HX), off);
+                    off = fma(cc.cyl, (C)pv(e - S::HX), off);
+                    off = fma(cc.cyh, (C)pv(e + S::HX), off);
                   }
-                  off = fma(k > 0 ? zl_ : T(0), lo, off);
-                  off = fma(k < A.nz - 1 ? zh_ : T(0), hi, off);
-                  ap = fma(dg, v, -off);
+                  off = fma(k > 0 ? zl_ : C(0), (C)lo, off);
+                  off = fma(k < A.nz - 1 ? zh_ : C(0), (C)hi, off);
+                  ap = fma(dg, (C)v, -off);
                 }
                 pnew[idx] = v;
                 pap += (double)v * (double)ap;
@@ -375,17 +387,22 @@ __global__ void __launch_bounds__(kTmaThreads, 1) pcg_tma(const __grid_constant_
     const bool okB = pipeline(
         [&](const Chunk& c, T* base, uint64_t* bar) {
           fence_proxy_async_smem();
-          // MIXED updates the FP64 iterate in place with plain loads: no x box
-          mbar_arrive_expect_tx(bar, MIXED ? (uint32_t)(S::HALO + S::INTR) * sizeof(T) : S::BYTES_B);
+          // MIXED updates the FP64 x and r in place with plain loads: only the
+          // FP32 p box is staged
+          mbar_arrive_expect_tx(bar, MIXED ? (uint32_t)S::HALO * sizeof(T) : S::BYTES_B);
           const int hx = c.i0 - S::XO, hy = c.j0 - S::OY, hz = c.z0 - 1;
           if constexpr (S::D3) {
             tma_load_3d(base, pnew_map, hx, hy, hz, bar);
-            if constexpr (!MIXED) tma_load_3d(base + S::HALO_P, &TP.maps.x_int, c.i0, c.j0, c.z0, bar);
-            tma_load_3d(base + S::HALO_P + S::INTR_P, &TP.maps.r_int, c.i0, c.j0, c.z0, bar);
+            if constexpr (!MIXED) {
+              tma_load_3d(base + S::HALO_P, &TP.maps.x_int, c.i0, c.j0, c.z0, bar);
+              tma_load_3d(base + S::HALO_P + S::INTR_P, &TP.maps.r_int, c.i0, c.j0, c.z0, bar);
+            }
           } else {
             tma_load_2d(base, pnew_map, hx, hz, bar);
-            if constexpr (!MIXED) tma_load_2d(base + S::HALO_P, &TP.maps.x_int, c.i0, c.z0, bar);
-            tma_load_2d(base + S::HALO_P + S::INTR_P, &TP.maps.r_int, c.i0, c.z0, bar);
+            if constexpr (!MIXED) {
+              tma_load_2d(base + S::HALO_P, &TP.maps.x_int, c.i0, c.z0, bar);
+              tma_load_2d(base + S::HALO_P + S::INTR_P, &TP.maps.r_int, c.i0, c.z0, bar);
+            }
           }
         },
         [&](const Chunk& c, T* base) {
@@ -407,43 +424,54 @@ __global__ void __launch_bounds__(kTmaThreads, 1) pcg_tma(const __grid_constant_
             int q = col + IPL * kb;
             int64_t idx = i + (int64_t)A.nx * (j + (int64_t)A.ny * (c.z0 + kb));
             const int64_t pstride = (int64_t)A.nx * A.ny;
-            ColCoef<T> cc;
-            if constexpr (!FACE) cc = column_coef(A, i, j);
+            ColCoef<C> cc;
+            if constexpr (!FACE) cc = column_coef(AC, i, j);
             for (int kk = kb; kk < ke; ++kk, e += PL, q += IPL, idx += pstride) {
               const int k = c.z0 + kk;
               const T v = pb[e];
-              T ap, inv;
+              C ap, inv;
               if constexpr (FACE) {
-                const Coef<T> cf = face_coef(A, i, j, k);
-                ap = apply_coef(cf, v, pb[e - 1], pb[e + 1], S::D3 ? pb[e - S::HX] : T(0),
-                                S::D3 ? pb[e + S::HX] : T(0), pb[e - PL], pb[e + PL]);
-                inv = __ldg(P.invd + idx);
+                const Coef<C> cf = face_coef(AC, i, j, k);
+                ap = apply_coef(cf, (C)v, (C)pb[e - 1], (C)pb[e + 1],
+                                S::D3 ? (C)pb[e - S::HX] : C(0), S::D3 ? (C)pb[e + S::HX] : C(0),
+                                (C)pb[e - PL], (C)pb[e + PL]);
+                if constexpr (MIXED) inv = cf.inv;
+                else inv = __ldg(P.invd + idx);
               } else if (cc.has_ref && k == cc.ref_k) {
-                ap = v;
-                inv = T(1);
+                ap = (C)v;
+                inv = C(1);
               } else {
-                const T zl_ = __ldg(A.tz + k), zh_ = __ldg(A.tz + k + 1);
-                const T dg = (cc.sxy + zl_) + zh_;
-                T off = cc.cxl * pb[e - 1];
-                off = fma(cc.cxh, pb[e + 1], off);
+                const C zl_ = __ldg(AC.tz + k), zh_ = __ldg(AC.tz + k + 1);
+                const C dg = (cc.sxy + zl_) + zh_;
+                C off = cc.cxl * (C)pb[e - 1];
+                off = fma(cc.cxh, (C)pb[e + 1], off);
                 if (S::D3) {
-                  off = fma(cc.cyl, pb[e - S::HX], off);
-                  off = fma(cc.cyh, pb[e + S::HX], off);
+                  off = fma(cc.cyl, (C)pb[e - S::HX], off);
+                  off = fma(cc.cyh, (C)pb[e + S::HX], off);
                 }
-                off = fma(k > 0 ? zl_ : T(0), pb[e - PL], off);
-                off = fma(k < A.nz - 1 ? zh_ : T(0), pb[e + PL], off);
-                ap = fma(dg, v, -off);
+                off = fma(k > 0 ? zl_ : C(0), (C)pb[e - PL], off);
+                off = fma(k < A.nz - 1 ? zh_ : C(0), (C)pb[e + PL], off);
+                ap = fma(dg, (C)v, -off);
                 inv = rcp_rn(dg);
               }
-              if constexpr (MIXED) P.x64[idx] = fma(alpha, (double)v, P.x64[idx]);
-              else P.x[idx] = fma(talpha, v, xb[q]);
-              const T rn = fma(-talpha, ap, rb[q]);
-              P.r[idx] = rn;
-              const T zn = inv * rn;
-              P.z[idx] = zn;
-              const double rd = (double)rn;
-              ab[0] += rd * rd;
-              ab[1] += rd * (double)zn;
+              if constexpr (MIXED) {
+                P.x64[idx] = fma(alpha, (double)v, P.x64[idx]);
+                const double rn = fma(-alpha, ap, P.r64[idx]);
+                P.r64[idx] = rn;
+                const T zn = (T)(inv * rn);
+                P.z[idx] = zn;
+                ab[0] += rn * rn;
+                ab[1] += rn * (double)zn;
+              } else {
+                P.x[idx] = fma(talpha, v, xb[q]);
+                const T rn = fma(-talpha, ap, rb[q]);
+                P.r[idx] = rn;
+                const T zn = inv * rn;
+                P.z[idx] = zn;
+                const double rd = (double)rn;
+                ab[0] += rd * rd;
+                ab[1] += rd * (double)zn;
+              }
             }
           }
         });

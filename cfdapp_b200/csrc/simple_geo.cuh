@@ -1,8 +1,12 @@
-// Geometry and boundary data of a uniform Cartesian SIMPLE case, evaluated
-// with the reference's own expressions (MeshGrading.cpp AxisSpacing::uniform
-// center/node/width; MeshGeometry.cpp:513-552, 1047-1140, 197-284) so the
-// stage kernels reproduce the reference's arithmetic.  Shared by host and
-// device; passed to kernels by value.
+// Geometry and boundary data of a Cartesian SIMPLE case, evaluated with the
+// reference's own expressions (MeshGrading.cpp AxisSpacing::uniform /
+// fromNodes center/node/width; MeshGeometry.cpp:513-552, 1047-1140, 197-284)
+// so the stage kernels reproduce the reference's arithmetic.  An axis is
+// either uniform (spacing delta, createCartesian2D/3D) or given by its node
+// coordinates (a rectilinear mesh: createRectilinear2D / createGraded2D,
+// MeshGeometry.hpp:228-240), in which case cell widths, face areas and cell
+// volumes vary along it.  Shared by host and device; passed to kernels by
+// value.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -30,7 +34,10 @@ struct SGeo {
   int n[3];
   int64_t stride[3];
   double delta[3];
-  double area[3];
+  // node coordinates of a non-uniform axis (n[a] + 1 values; host or device
+  // memory to match where the SGeo is used), null for a uniform axis
+  const double* node[3];
+  double area[3];  // face areas and cell volume of an all-uniform grid
   double vol;
   int64_t nc, nf;
   int64_t foff[3];
@@ -43,10 +50,31 @@ struct SGeo {
 };
 
 __host__ __device__ inline double g_center(const SGeo& G, int a, int64_t i) {
-  return ((double)i + 0.5) * G.delta[a];
+  return G.node[a] ? 0.5 * (G.node[a][i] + G.node[a][i + 1]) : ((double)i + 0.5) * G.delta[a];
 }
 __host__ __device__ inline double g_node(const SGeo& G, int a, int64_t i) {
-  return (double)i * G.delta[a];
+  return G.node[a] ? G.node[a][i] : (double)i * G.delta[a];
+}
+__host__ __device__ inline double g_width(const SGeo& G, int a, int64_t i) {
+  return G.node[a] ? G.node[a][i + 1] - G.node[a][i] : G.delta[a];
+}
+__host__ __device__ inline bool g_uniform(const SGeo& G) {
+  return !G.node[0] && !G.node[1] && !G.node[2];
+}
+// Area of the axis-a faces of cell ijk: the widths of the other axes (a 2D
+// x-face's area vector is (+-height, 0), a y-face's (0, +-width)).
+__host__ __device__ inline double g_area(const SGeo& G, int a, const int ijk[3]) {
+  if (g_uniform(G)) return G.area[a];
+  if (G.dim == 2) return g_width(G, 1 - a, ijk[1 - a]);
+  if (a == 0) return g_width(G, 1, ijk[1]) * g_width(G, 2, ijk[2]);
+  if (a == 1) return g_width(G, 0, ijk[0]) * g_width(G, 2, ijk[2]);
+  return g_width(G, 0, ijk[0]) * g_width(G, 1, ijk[1]);
+}
+// Volume of cell ijk (width x height [x depth]).
+__host__ __device__ inline double g_vol(const SGeo& G, const int ijk[3]) {
+  if (g_uniform(G)) return G.vol;
+  const double v = g_width(G, 0, ijk[0]) * g_width(G, 1, ijk[1]);
+  return G.dim == 2 ? v : v * g_width(G, 2, ijk[2]);
 }
 // Internal face at coordinate f along a (owner f-1, neighbour f).
 __host__ __device__ inline double g_dpf(const SGeo& G, int a, int64_t f) {
@@ -78,6 +106,13 @@ __host__ __device__ inline void g_coords(const SGeo& G, int64_t c, int ijk[3]) {
   ijk[0] = (int)(c % G.n[0]);
   ijk[1] = (int)((c / G.n[0]) % G.n[1]);
   ijk[2] = (int)(c / ((int64_t)G.n[0] * G.n[1]));
+}
+
+__host__ __device__ inline double g_vol_c(const SGeo& G, int64_t c) {
+  if (g_uniform(G)) return G.vol;
+  int ijk[3];
+  g_coords(G, c, ijk);
+  return g_vol(G, ijk);
 }
 
 // Global id of the face of cell ijk on axis a, side s.
@@ -125,6 +160,14 @@ __host__ __device__ inline FaceInfo g_face_decode(const SGeo& G, int64_t id) {
   fi.high = (fi.f < G.n[fi.a]) ? base : -1;
   fi.low = (fi.f > 0) ? base - G.stride[fi.a] : -1;
   return fi;
+}
+
+// Area of a face given its decoded info (from the cell on either side).
+__host__ __device__ inline double g_face_area(const SGeo& G, const FaceInfo& fi) {
+  if (g_uniform(G)) return G.area[fi.a];
+  int ijk[3];
+  g_coords(G, fi.high >= 0 ? fi.high : fi.low, ijk);
+  return g_area(G, fi.a, ijk);
 }
 
 __host__ __device__ inline int g_vbc_prescribed(int t) {

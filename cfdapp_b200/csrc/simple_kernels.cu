@@ -69,7 +69,7 @@ __global__ void k_assemble_momentum(SGeo G, double mu, int scheme, int comp, con
 
 // d = V / aP (PressureCorrectionEquation.cpp:103-114).
 __global__ void k_response(SGeo G, const double* diag, double* d) {
-  GRID_STRIDE(c, G.nc) d[c] = ops::response(G, diag[c]);
+  GRID_STRIDE(c, G.nc) d[c] = ops::response(G, diag[c], c);
 }
 
 // Rhie-Chow correction of the internal faces (RhieChow.cpp:17-51).

@@ -1,5 +1,5 @@
-// Per-cell and per-face operations of the SIMPLE stages on uniform Cartesian
-// grids, shared by the single-case kernels (simple_kernels.cu) and the batched
+// Per-cell and per-face operations of the SIMPLE stages on Cartesian grids
+// (uniform or rectilinear), shared by the single-case kernels (simple_kernels.cu) and the batched
 // persistent kernels (batch_stages.cu), so that a stage computes the same
 // value for a cell whichever of them runs it.
 //
@@ -21,7 +21,7 @@ namespace ops {
 __device__ inline double mass_flux(const SGeo& G, double rho, const double* const U[3], int64_t id) {
   const FaceInfo fi = g_face_decode(G, id);
   const int a = fi.a;
-  double ua, sa = G.area[a];
+  double ua, sa = g_face_area(G, fi);
   if (fi.low >= 0 && fi.high >= 0) {
     ua = g_interp_v(G, a, fi.f, U[a][fi.low], U[a][fi.high]);
   } else if (fi.low < 0) {
@@ -70,13 +70,13 @@ __device__ inline void gg_sweep(const SGeo& G, const double* phi, const double* 
       corr[a][1 - s] = fv[of] + correction;
       has[a][1 - s] = 1;
     }
-  const double inv = 1.0 / G.vol;
+  const double inv = 1.0 / g_vol(G, ijk);
   for (int a = 0; a < G.dim; ++a) {
     double sum = 0.0;
     for (int s = 0; s < 2; ++s) {
       const int64_t f = g_face_of(G, ijk, a, s);
       const double val = has[a][s] ? corr[a][s] : fv[f];
-      const double sf = (s == 0) ? -G.area[a] : G.area[a];
+      const double sf = (s == 0) ? -g_area(G, a, ijk) : g_area(G, a, ijk);
       sum += sf * val;
     }
     out[a][c] = sum * inv;
@@ -88,7 +88,7 @@ __device__ inline void velocity_gradient(const SGeo& G, const double* uc, int co
                                          double* const grad[3], int64_t c) {
   int ijk[3];
   g_coords(G, c, ijk);
-  const double inv = 1.0 / G.vol;
+  const double inv = 1.0 / g_vol(G, ijk);
   for (int a = 0; a < G.dim; ++a) {
     double sum = 0.0;
     for (int s = 0; s < 2; ++s) {
@@ -102,7 +102,7 @@ __device__ inline void velocity_gradient(const SGeo& G, const double* uc, int co
         const int64_t hi = s == 0 ? c : c + G.stride[a];
         val = g_interp_v(G, a, f, uc[lo], uc[hi]);
       }
-      const double sf = (s == 0) ? -G.area[a] : G.area[a];
+      const double sf = (s == 0) ? -g_area(G, a, ijk) : g_area(G, a, ijk);
       sum += sf * val;
     }
     grad[a][c] = sum * inv;
@@ -184,7 +184,7 @@ __device__ inline void assemble_momentum(const SGeo& G, double mu, int scheme, i
         const double phiB = g_vbc_value(G, patch, comp, uc[c]);
         const SideGeo& q = G.side[a][s];
         if (g_vbc_prescribed(G.vtype[patch]) && q.valid && q.stencil_ok) {
-          const double ga = mu * G.area[a];
+          const double ga = mu * g_area(G, a, ijk);
           const double cP = q.h2 / (q.h1 * (q.h2 - q.h1));
           const double cF = q.h1 / (q.h2 * (q.h2 - q.h1));
           const double cB = (1.0 / q.h1) + (1.0 / q.h2);
@@ -196,14 +196,14 @@ __device__ inline void assemble_momentum(const SGeo& G, double mu, int scheme, i
           rh += (ga * cB) * phiB;
           o[2 * a + (1 - s)] += -(ga * cF);
         } else {
-          const double coef = mu * G.area[a] / g_dbnd(G, a, s);
+          const double coef = mu * g_area(G, a, ijk) / g_dbnd(G, a, s);
           dg += coef;
           rh += coef * phiB;
         }
       } else {
         const int64_t f = ijk[a] + s;
         const double muf = g_interp_s(G, a, f, mu, mu);
-        const double D = muf * G.area[a] / g_dpn(G, a, f);
+        const double D = muf * g_area(G, a, ijk) / g_dpn(G, a, f);
         dg += D;
         o[2 * a + s] += -D;
       }
@@ -234,7 +234,7 @@ __device__ inline void assemble_momentum(const SGeo& G, double mu, int scheme, i
         else rh += corr;
       }
     }
-  rh += -G.vol * gradPc[c];
+  rh += -g_vol(G, ijk) * gradPc[c];
   if (alpha != 1.0) {
     const double extra = dg * factor;
     dg += extra;
@@ -246,12 +246,14 @@ __device__ inline void assemble_momentum(const SGeo& G, double mu, int scheme, i
 }
 
 // d = V / aP (PressureCorrectionEquation.cpp:103-114).
-__device__ inline double response(const SGeo& G, double aP) { return G.vol / aP; }
+__device__ inline double response(const SGeo& G, double aP, int64_t c) {
+  return g_vol_c(G, c) / aP;
+}
 
-__device__ inline double pface_internal(const SGeo& G, double rho, int a, int64_t f, double dP,
+__device__ inline double pface_internal(const SGeo& G, double rho, const FaceInfo& fi, double dP,
                                         double dN) {
-  const double dFace = g_interp_s(G, a, f, dP, dN);
-  return rho * G.area[a] * dFace / g_dpn(G, a, f);
+  const double dFace = g_interp_s(G, fi.a, fi.f, dP, dN);
+  return rho * g_face_area(G, fi) * dFace / g_dpn(G, fi.a, fi.f);
 }
 
 // Rhie-Chow correction of one internal face (RhieChow.cpp:17-51); boundary
@@ -262,7 +264,7 @@ __device__ inline void rhie_chow(const SGeo& G, double rho, double alpha, const 
   const FaceInfo fi = g_face_decode(G, id);
   if (fi.low < 0 || fi.high < 0) return;
   const int a = fi.a;
-  const double coupling = pface_internal(G, rho, a, fi.f, d[a][fi.low], d[a][fi.high]);
+  const double coupling = pface_internal(G, rho, fi, d[a][fi.low], d[a][fi.high]);
   const double dvec = g_center(G, a, fi.f) - g_center(G, a, fi.f - 1);
   const double gf = g_interp_v(G, a, fi.f, gp[a][fi.low], gp[a][fi.high]);
   const double cmi = (p[fi.high] - p[fi.low]) - (gf * dvec);
@@ -272,11 +274,11 @@ __device__ inline void rhie_chow(const SGeo& G, double rho, double alpha, const 
 // p' face coefficient (pressureCorrectionFaceCoupling, PressureCorrectionEquation.cpp:146-179).
 __device__ inline double pprime_face(const SGeo& G, double rho, const double* const d[3], int64_t id) {
   const FaceInfo fi = g_face_decode(G, id);
-  if (fi.low >= 0 && fi.high >= 0) return pface_internal(G, rho, fi.a, fi.f, d[fi.a][fi.low], d[fi.a][fi.high]);
+  if (fi.low >= 0 && fi.high >= 0) return pface_internal(G, rho, fi, d[fi.a][fi.low], d[fi.a][fi.high]);
   const int side = fi.low < 0 ? 0 : 1;
   const int64_t owner = side == 0 ? fi.high : fi.low;
   return (G.ptype[2 * fi.a + side] == PBC_FIXED_VALUE)
-             ? rho * G.area[fi.a] * d[fi.a][owner] / g_dbnd(G, fi.a, side)
+             ? rho * g_face_area(G, fi) * d[fi.a][owner] / g_dbnd(G, fi.a, side)
              : 0.0;
 }
 

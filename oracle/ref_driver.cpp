@@ -22,7 +22,8 @@
 //          [scheme=upwind|central|lud|quick] [flux=auto|linear|rhiechow]
 //          [mabs=1e-10] [mrel=1e-8] [mmax=500]
 //          [psolver=cg|bicgstab] [ppre=jacobi|none] [pabs=0] [prel=1e-8] [pmax=5000]
-//          [mbackend=cpu|gpu] [pbackend=cpu|gpu] [out=DIR]
+//          [mbackend=cpu|gpu] [pbackend=cpu|gpu] [gradex=R gradey=R cluster=both|start|end]
+//          [out=DIR]
 //       the reference SIMPLE::solve (SIMPLE.cpp:148) on a uniform Cartesian
 //       lid-driven cavity (Wall x3 + MovingWall{lid,0}) or channel (Inlet
 //       {inlet,0} left, Outlet right, Walls; pressure FixedValue(0) at the
@@ -62,6 +63,7 @@
 #include "cfd/fields/VectorField.hpp"
 #include "cfd/gpu/GPUExecutionStats.hpp"
 #include "cfd/mesh/MeshGeometry.hpp"
+#include "cfd/mesh/MeshGrading.hpp"
 #include "cfd/physics/FluidProperties.hpp"
 #include "cfd/pressure_velocity/PressureCorrectionEquation.hpp"
 #include "cfd/pressure_velocity/SIMPLE.hpp"
@@ -133,6 +135,22 @@ mesh::Mesh makeMesh(int dim, long long nx, long long ny, long long nz, double lx
                     double lz) {
   if (dim == 3) return mesh::MeshGeometry::createCartesian3D(nx, ny, nz, lx, ly, lz);
   return mesh::MeshGeometry::createCartesian2D(nx, ny, lx, ly);
+}
+
+// gradex=R / gradey=R (geometric ratio, cluster=both|start|end): the 2D
+// mesh of MeshGeometry::createGraded2D (MeshGeometry.hpp:236-240).
+mesh::AxisGrading grading(const Args& a, const std::string& key) {
+  mesh::AxisGrading g;
+  const double ratio = getd(a, key, 1.0);
+  if (ratio != 1.0) {
+    g.type = mesh::GradingType::Geometric;
+    g.ratio = ratio;
+    const std::string c = get(a, "cluster", "both");
+    g.cluster = c == "start" ? mesh::GradingCluster::Start
+                : c == "end" ? mesh::GradingCluster::End
+                             : mesh::GradingCluster::Both;
+  }
+  return g;
 }
 
 // The isolated p' matrix through the reference's own assembly
@@ -340,7 +358,10 @@ int runSimple(const Args& a) {
   const double lx = getd(a, "lx", 1.0), ly = getd(a, "ly", 1.0), lz = getd(a, "lz", 1.0);
   const std::string out = get(a, "out", "");
   const std::string flow = get(a, "flow", "cavity");
-  const mesh::Mesh m = makeMesh(dim, nx, ny, nz, lx, ly, lz);
+  const bool graded = dim == 2 && (a.count("gradex") || a.count("gradey"));
+  const mesh::Mesh m = graded ? mesh::MeshGeometry::createGraded2D(nx, ny, lx, ly, grading(a, "gradex"),
+                                                                    grading(a, "gradey"))
+                              : makeMesh(dim, nx, ny, nz, lx, ly, lz);
   const Index cells = m.numberOfCells();
   const physics::FluidProperties fluid(getd(a, "rho", 1.0), getd(a, "mu", 0.01));
 
@@ -431,6 +452,14 @@ int runSimple(const Args& a) {
       hist.push_back(r.continuityHistory[k]);
     }
     writeBin(out + "/hist.bin", hist);
+    if (graded) {  // the node coordinates of each axis (the generating vertex grid)
+      const mesh::StructuredGrid* sg = m.structuredGrid();
+      std::vector<double> xn(nx + 1), yn(ny + 1);
+      for (long long i = 0; i <= nx; ++i) xn[i] = sg->vertex(i, 0).x;
+      for (long long j = 0; j <= ny; ++j) yn[j] = sg->vertex(0, j).y;
+      writeBin(out + "/x_nodes.bin", xn);
+      writeBin(out + "/y_nodes.bin", yn);
+    }
   }
   return 0;
 }

@@ -57,7 +57,10 @@ def test_isolated_fp32_refined_reaches_fp64_tolerance(ctx, dim, n):
     # true residual recomputed on the CPU from the returned x
     ax = O.stencil_apply(case, diag, off, res.solution)
     assert np.linalg.norm(b - ax) / np.linalg.norm(b) <= 1.01e-8
-    assert _rel(res.solution, ref.solution) <= 1e-6
+    # two iterates that each meet rel-res 1e-8 differ by at most about
+    # cond(A) x 2e-8 (cond ~ 1e3 on these grids); the FP64 solves follow the
+    # same iterates and meet 1e-9, the mixed one takes its own path
+    assert _rel(res.solution, ref.solution) <= 2e-5
 
 
 @pytest.mark.parametrize("dim,n", [(2, 512), (3, 64)])
@@ -78,7 +81,7 @@ def test_mixed_precision_keeps_one_krylov_space(ctx, dim, n):
     ax = O.stencil_apply(case, diag, off, r32.solution)
     assert np.linalg.norm(b - ax) / np.linalg.norm(b) <= 1.01e-8
     assert r32.residual_history[-1] == pytest.approx(r32.final_residual, rel=1e-12)
-    assert _rel(r32.solution, r64.solution) <= 1e-6
+    assert _rel(r32.solution, r64.solution) <= 1e-4  # cond(A) x 2e-8 at these sizes
     # FP32 vectors: fewer bytes per iteration than the FP64 solve
     assert r32.krylov_bytes / r32.iterations < 0.7 * r64.krylov_bytes / r64.iterations
 
@@ -100,7 +103,7 @@ def test_mixed_precision_on_face_coefficients(ctx, dim, n):
     assert res.status == "Converged"
     ax = O.stencil_apply(case, diag, off, res.solution)
     assert np.linalg.norm(rhs - ax) / np.linalg.norm(rhs) <= 1.01e-8
-    assert _rel(res.solution, ref.solution) <= 1e-6
+    assert _rel(res.solution, ref.solution) <= 2e-5  # the residual bound, as above
 
 
 @pytest.mark.parametrize("dim,n", [(2, 40), (3, 12)])
