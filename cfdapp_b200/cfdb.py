@@ -448,7 +448,7 @@ FACE_FLUX = {"linear": 0, "rhie_chow": 1, "rhiechow": 1, "automatic": 2, "auto":
 class _SimpleCase(C.Structure):
     _fields_ = [("grid", _Grid), ("vbc_type", C.c_int * 6), ("vbc_value", (C.c_double * 3) * 6),
                 ("pbc_type", C.c_int * 6), ("pbc_value", C.c_double * 6), ("rho", C.c_double),
-                ("mu", C.c_double)]
+                ("mu", C.c_double), ("nodes", C.POINTER(C.c_double) * 3)]
 
 
 class _SimpleSettings(C.Structure):
@@ -470,7 +470,8 @@ class _SimpleResult(C.Structure):
 
 @dataclass
 class SimpleCase:
-    """A uniform Cartesian case (MeshGeometry::createCartesian2D/3D + BCs + fluid)."""
+    """A Cartesian case (MeshGeometry::createCartesian2D/3D, or with per-axis
+    node coordinates createRectilinear2D / createGraded2D) + BCs + fluid."""
     dim: int
     n: tuple
     length: tuple = (1.0, 1.0, 1.0)
@@ -478,6 +479,7 @@ class SimpleCase:
     pbc: tuple = ()     # per patch: (type, value)
     rho: float = 1.0
     mu: float = 0.01
+    nodes: tuple = ()   # per axis: n+1 node coordinates, or None for a uniform axis
 
     @staticmethod
     def cavity(dim: int, n: int, lid: float = 1.0, mu: float = 0.01, rho: float = 1.0):
@@ -517,6 +519,17 @@ class SimpleCase:
             cs.pbc_value[q] = float(pv)
         cs.rho = self.rho
         cs.mu = self.mu
+        self._node_arrays = []  # kept alive with the case while the struct is in use
+        for a in range(3):
+            nd = self.nodes[a] if a < len(self.nodes) else None
+            if nd is None:
+                cs.nodes[a] = None
+            else:
+                arr = np.ascontiguousarray(nd, dtype=np.float64)
+                if arr.size != self.n[a] + 1:
+                    raise CfdbError(f"axis {a}: {arr.size} node coordinates for {self.n[a]} cells")
+                self._node_arrays.append(arr)
+                cs.nodes[a] = _dp(arr)
         return cs
 
 

@@ -551,6 +551,9 @@ cfdb_status cfdb_batch_create(cfdb_context* ctx, int ncases, const cfdb_simple_c
     cfdb_status rc = simple_validate(ctx, &cases[k], st);
     if (rc != CFDB_OK) return rc;
     if (cases[k].grid.dim != dim) return set_error(ctx, CFDB_ERR_INVALID_ARGUMENT, "a batch holds one dimension");
+    for (int a = 0; a < 3; ++a)
+      if (cases[k].nodes[a])
+        return set_error(ctx, CFDB_ERR_UNSUPPORTED, "a batch holds uniform grids only");
   }
   if (st->max_outer < 1 || !(st->alpha_u > 0.0) || st->alpha_u > 1.0 || !(st->alpha_p > 0.0) ||
       st->alpha_p > 1.0 ||

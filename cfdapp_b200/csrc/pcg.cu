@@ -469,16 +469,22 @@ cfdb_status launch_pcg_tma(cfdb_context* ctx, PcgParams<T>& P) {
   const uint32_t* halo = S::D3 ? halo3 : halo2;
   const uint32_t* intr = S::D3 ? intr3 : intr2;
   const int es = (int)sizeof(T);
+  // MIXED: x and r are the FP64 x64, r64 (interior boxes of doubles)
+  const CUtensorMapDataType dti = MIXED ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : dt;
+  const int esi = MIXED ? 8 : es;
+  void* xint = MIXED ? (void*)P.x64 : (void*)P.x;
+  void* rint = MIXED ? (void*)P.r64 : (void*)P.r;
   if (!encode_tensor_map(&TP.maps.z_halo, dt, es, rank, P.z, dims, halo) ||
       !encode_tensor_map(&TP.maps.p0_halo, dt, es, rank, P.p0, dims, halo) ||
       !encode_tensor_map(&TP.maps.p1_halo, dt, es, rank, P.p1, dims, halo) ||
-      // MIXED keeps x in FP64 and updates it with plain loads: its map is
-      // never used and points at r only to stay well formed
-      !encode_tensor_map(&TP.maps.x_int, dt, es, rank, MIXED ? P.r : P.x, dims, intr) ||
-      !encode_tensor_map(&TP.maps.r_int, dt, es, rank, P.r, dims, intr))
+      !encode_tensor_map(&TP.maps.x_int, dti, esi, rank, xint, dims, intr) ||
+      !encode_tensor_map(&TP.maps.r_int, dti, esi, rank, rint, dims, intr))
     return set_error(ctx, CFDB_ERR_CUDA, "cuTensorMapEncodeTiled rejected a p' tensor map");
   auto kernel = P.A.fx ? pcg_tma<T, S, true, MIXED> : pcg_tma<T, S, false, MIXED>;
-  const size_t smem = sizeof(T) * (size_t)S::STAGE * 2;
+  // stage: MIXED carries FP64 x and r boxes (2 x INTR_P doubles after the halo)
+  const size_t stage_words = MIXED ? (size_t)std::max(2 * S::HALO_P, S::HALO_P + 4 * S::INTR_P)
+                                   : (size_t)S::STAGE;
+  const size_t smem = sizeof(T) * stage_words * 2;
   CFDB_CUDA(ctx, cudaFuncSetAttribute((const void*)kernel,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;

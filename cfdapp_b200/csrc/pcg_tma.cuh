@@ -126,6 +126,12 @@ __global__ void __launch_bounds__(kTmaThreads, 1) pcg_tma(const __grid_constant_
   static_assert(!MIXED || sizeof(T) == 4, "the mixed-precision solve stores p and z in FP32");
   // coefficients and stencil arithmetic: FP64 in the mixed solve, else T
   using C = typename std::conditional<MIXED, double, T>::type;
+  // sweep B stage of the mixed solve: the FP32 p halo box, then FP64 x and r
+  // interior boxes (each 128-byte aligned); stage size in T words
+  constexpr int XOFF = S::HALO_P, ROFF = S::HALO_P + 2 * S::INTR_P;
+  constexpr int STG = MIXED ? (2 * S::HALO_P > ROFF + 2 * S::INTR_P ? 2 * S::HALO_P
+                                                                     : ROFF + 2 * S::INTR_P)
+                            : S::STAGE;
   extern __shared__ __align__(128) unsigned char smem_tma[];
   T* stage_mem = reinterpret_cast<T*>(smem_tma);
   __shared__ __align__(8) uint64_t bars[2];
@@ -165,7 +171,7 @@ __global__ void __launch_bounds__(kTmaThreads, 1) pcg_tma(const __grid_constant_
       Chunk cn;
       const bool issued = ld.template next<S::TZ>(cs, A.nz, S::TX, S::TY, B, cn);
       if (issued && tid == 0)
-        load(cn, stage_mem + (size_t)(st ^ 1) * S::STAGE, &bars[st ^ 1]);
+        load(cn, stage_mem + (size_t)(st ^ 1) * STG, &bars[st ^ 1]);
       const bool ok = mbar_wait(&bars[st], parity[st], P.sync.error, P.sync.timeout_ns);
       if (__syncthreads_or(!ok)) {
         if (tid == 0) {
@@ -175,7 +181,7 @@ __global__ void __launch_bounds__(kTmaThreads, 1) pcg_tma(const __grid_constant_
         return false;
       }
       parity[st] ^= 1u;
-      body(cc, stage_mem + (size_t)st * S::STAGE);
+      body(cc, stage_mem + (size_t)st * STG);
       __syncthreads();
       ++q;
     }
@@ -387,22 +393,20 @@ __global__ void __launch_bounds__(kTmaThreads, 1) pcg_tma(const __grid_constant_
     const bool okB = pipeline(
         [&](const Chunk& c, T* base, uint64_t* bar) {
           fence_proxy_async_smem();
-          // MIXED updates the FP64 x and r in place with plain loads: only the
-          // FP32 p box is staged
-          mbar_arrive_expect_tx(bar, MIXED ? (uint32_t)S::HALO * sizeof(T) : S::BYTES_B);
+          // MIXED: the x and r boxes are FP64 (maps over x64 and r64)
+          mbar_arrive_expect_tx(bar, MIXED ? (uint32_t)(S::HALO * sizeof(T) + 2 * S::INTR * sizeof(double))
+                                           : S::BYTES_B);
           const int hx = c.i0 - S::XO, hy = c.j0 - S::OY, hz = c.z0 - 1;
+          T* xdst = base + (MIXED ? XOFF : S::HALO_P);
+          T* rdst = base + (MIXED ? ROFF : S::HALO_P + S::INTR_P);
           if constexpr (S::D3) {
             tma_load_3d(base, pnew_map, hx, hy, hz, bar);
-            if constexpr (!MIXED) {
-              tma_load_3d(base + S::HALO_P, &TP.maps.x_int, c.i0, c.j0, c.z0, bar);
-              tma_load_3d(base + S::HALO_P + S::INTR_P, &TP.maps.r_int, c.i0, c.j0, c.z0, bar);
-            }
+            tma_load_3d(xdst, &TP.maps.x_int, c.i0, c.j0, c.z0, bar);
+            tma_load_3d(rdst, &TP.maps.r_int, c.i0, c.j0, c.z0, bar);
           } else {
             tma_load_2d(base, pnew_map, hx, hz, bar);
-            if constexpr (!MIXED) {
-              tma_load_2d(base + S::HALO_P, &TP.maps.x_int, c.i0, c.z0, bar);
-              tma_load_2d(base + S::HALO_P + S::INTR_P, &TP.maps.r_int, c.i0, c.z0, bar);
-            }
+            tma_load_2d(xdst, &TP.maps.x_int, c.i0, c.z0, bar);
+            tma_load_2d(rdst, &TP.maps.r_int, c.i0, c.z0, bar);
           }
         },
         [&](const Chunk& c, T* base) {
@@ -455,8 +459,10 @@ __global__ void __launch_bounds__(kTmaThreads, 1) pcg_tma(const __grid_constant_
                 inv = rcp_rn(dg);
               }
               if constexpr (MIXED) {
-                P.x64[idx] = fma(alpha, (double)v, P.x64[idx]);
-                const double rn = fma(-alpha, ap, P.r64[idx]);
+                const double* xb64 = reinterpret_cast<const double*>(base + XOFF);
+                const double* rb64 = reinterpret_cast<const double*>(base + ROFF);
+                P.x64[idx] = fma(alpha, (double)v, xb64[q]);
+                const double rn = fma(-alpha, ap, rb64[q]);
                 P.r64[idx] = rn;
                 const T zn = (T)(inv * rn);
                 P.z[idx] = zn;

@@ -118,9 +118,17 @@ cfdb_status cfdb_write_results(const cfdb_simple_case* cs, const double* u, cons
         (dim == 3 && !std::isfinite(w[c])))
       return CFDB_OK;  // no field files for a non-finite result
 
-  auto cx = [&](int64_t i) { return ((double)i + 0.5) * hx; };
-  auto cy = [&](int64_t j) { return ((double)j + 0.5) * hy; };
-  auto cz = [&](int64_t k) { return ((double)k + 0.5) * hz; };
+  // cell centres and nodes as AxisSpacing computes them (uniform: (i + 0.5)
+  // delta and i delta; from node coordinates: 0.5 (n_i + n_i+1) and n_i)
+  const double* const* nd = cs->nodes;
+  auto cx = [&](int64_t i) { return nd[0] ? 0.5 * (nd[0][i] + nd[0][i + 1]) : ((double)i + 0.5) * hx; };
+  auto cy = [&](int64_t j) { return nd[1] ? 0.5 * (nd[1][j] + nd[1][j + 1]) : ((double)j + 0.5) * hy; };
+  auto cz = [&](int64_t k) {
+    return (dim == 3 && nd[2]) ? 0.5 * (nd[2][k] + nd[2][k + 1]) : ((double)k + 0.5) * hz;
+  };
+  auto nxp = [&](int64_t i) { return nd[0] ? nd[0][i] : (double)i * hx; };
+  auto nyp = [&](int64_t j) { return nd[1] ? nd[1][j] : (double)j * hy; };
+  auto nzp = [&](int64_t k) { return (dim == 3 && nd[2]) ? nd[2][k] : (double)k * hz; };
 
   // fields.csv
   {
@@ -170,12 +178,12 @@ cfdb_status cfdb_write_results(const cfdb_simple_case* cs, const double* u, cons
     for (int64_t k = 0; k < pz; ++k)
       for (int64_t j = 0; j < py; ++j)
         for (int64_t i = 0; i < px; ++i) {
-          o.real((double)i * hx);
+          o.real(nxp(i));
           o.ch(' ');
-          o.real((double)j * hy);
+          o.real(nyp(j));
           if (dim == 3) {
             o.ch(' ');
-            o.real((double)k * hz);
+            o.real(nzp(k));
             o.ch('\n');
           } else {
             o.text(" 0\n");

@@ -40,7 +40,12 @@ SideGeo side_geometry(const SGeo& G, int a, int s) {
   const int ip = (s == 0) ? 0 : n - 1;
   const int iF = (s == 0) ? 1 : n - 2;
   const double xb = (s == 0) ? g_node(G, a, 0) : g_node(G, a, n);
-  const double sfa = (s == 0) ? -G.area[a] : G.area[a];
+  // the boundary face's area vector (only its sign and scale enter); on a
+  // rectilinear mesh the first face of the side stands for all of them,
+  // whose quantities below differ from it at most in their last bits
+  const int ijk0[3] = {ip * (a == 0), ip * (a == 1), ip * (a == 2)};
+  const double area = g_area(G, a, ijk0);
+  const double sfa = (s == 0) ? -area : area;
   const double cP = g_center(G, a, ip), cF = g_center(G, a, iF);
   const double d = cF - cP;
   sg.L = std::fabs(d);
@@ -52,7 +57,7 @@ SideGeo side_geometry(const SGeo& G, int a, int s) {
   sg.tb = ((cP - xb) * sfa) / (inward * sfa);
   const double point = cP - (inward * sg.tb);
   sg.offset = point - xb;
-  const double normal = sfa * (1.0 / G.area[a]);
+  const double normal = sfa * (1.0 / area);
   sg.h1 = (xb - cP) * normal;
   sg.h2 = (xb - cF) * normal;
   sg.stencil_ok = (sg.h1 > 0.0) && (sg.h2 > sg.h1);
@@ -61,6 +66,8 @@ SideGeo side_geometry(const SGeo& G, int a, int s) {
   return sg;
 }
 
+// node[a]: node coordinates of axis a in the memory the SGeo will be used
+// from (host during construction), or null for a uniform axis.
 SGeo make_geo(const cfdb_simple_case& cs) {
   SGeo G;
   std::memset(&G, 0, sizeof(G));
@@ -70,7 +77,10 @@ SGeo make_geo(const cfdb_simple_case& cs) {
   G.stride[0] = 1;
   G.stride[1] = G.n[0];
   G.stride[2] = (int64_t)G.n[0] * G.n[1];
-  for (int a = 0; a < g.dim; ++a) G.delta[a] = g.len[a] / (double)g.n[a];
+  for (int a = 0; a < g.dim; ++a) {
+    G.node[a] = cs.nodes[a];
+    G.delta[a] = cs.nodes[a] ? 0.0 : g.len[a] / (double)g.n[a];
+  }
   if (g.dim == 2) {
     G.area[0] = G.delta[1];
     G.area[1] = G.delta[0];
@@ -170,6 +180,8 @@ struct cfdb_simple {
   cfdb_poperator* pop = nullptr;
   StencilWork work;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
+  std::vector<double> hnodes[3];  // node coordinates of non-uniform axes (host copy)
+  double* dnodes[3] = {nullptr, nullptr, nullptr};
 
   ~cfdb_simple() {
     for (double* q : owned) cudaFree(q);
@@ -178,6 +190,7 @@ struct cfdb_simple {
     cudaFree(d_pctype);
     cudaFree(d_pcvalue);
     cudaFree(flag);
+    for (double* q : dnodes) cudaFree(q);
     if (pop) cfdb_poperator_destroy(pop);
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
@@ -215,9 +228,15 @@ cfdb_status validate(cfdb_context* ctx, const cfdb_simple_case* cs, const cfdb_s
   if (!cs || !st) return set_error(ctx, CFDB_ERR_INVALID_ARGUMENT, "null case or settings");
   const cfdb_grid& g = cs->grid;
   if (g.dim != 2 && g.dim != 3) return set_error(ctx, CFDB_ERR_INVALID_ARGUMENT, "dim must be 2 or 3");
-  for (int a = 0; a < g.dim; ++a)
-    if (g.n[a] < 2 || g.n[a] > (1 << 20) || !(g.len[a] > 0.0))
+  for (int a = 0; a < g.dim; ++a) {
+    if (g.n[a] < 2 || g.n[a] > (1 << 20) || (!cs->nodes[a] && !(g.len[a] > 0.0)))
       return set_error(ctx, CFDB_ERR_INVALID_ARGUMENT, "each axis needs >= 2 cells and a positive length");
+    if (cs->nodes[a])
+      for (int64_t i = 0; i <= g.n[a]; ++i)
+        if (!std::isfinite(cs->nodes[a][i]) || (i > 0 && !(cs->nodes[a][i] > cs->nodes[a][i - 1])))
+          return set_error(ctx, CFDB_ERR_INVALID_ARGUMENT,
+                           "node coordinates must be finite and strictly increasing");
+  }
   if (!(cs->rho > 0.0) || !(cs->mu > 0.0) || !std::isfinite(cs->rho) || !std::isfinite(cs->mu))
     return set_error(ctx, CFDB_ERR_INVALID_ARGUMENT, "rho and mu must be finite and > 0");
   for (int q = 0; q < 2 * g.dim; ++q) {
@@ -438,7 +457,22 @@ cfdb_status cfdb_simple_create(cfdb_context* ctx, const cfdb_simple_case* cs,
   s->ctx = ctx;
   s->cs = *cs;
   s->st = *st;
-  s->G = make_geo(*cs);
+  for (int a = 0; a < 3; ++a) {  // the session keeps its own copy of the nodes
+    if (a < cs->grid.dim && cs->nodes[a]) {
+      s->hnodes[a].assign(cs->nodes[a], cs->nodes[a] + cs->grid.n[a] + 1);
+      s->cs.nodes[a] = s->hnodes[a].data();
+    } else {
+      s->cs.nodes[a] = nullptr;
+    }
+  }
+  s->G = make_geo(s->cs);  // host node pointers: the side geometry is computed here
+  for (int a = 0; a < 3; ++a)
+    if (s->cs.nodes[a]) {
+      const size_t bytes = sizeof(double) * s->hnodes[a].size();
+      CFDB_CUDA(ctx, cudaMalloc((void**)&s->dnodes[a], bytes));
+      CFDB_CUDA(ctx, cudaMemcpy(s->dnodes[a], s->hnodes[a].data(), bytes, cudaMemcpyHostToDevice));
+      s->G.node[a] = s->dnodes[a];  // the kernels read the device copy
+    }
   s->n = s->G.nc;
   s->nf = s->G.nf;
   s->face_flux = st->face_flux == CFDB_FLUX_AUTOMATIC ? (cs->grid.dim == 2 ? CFDB_FLUX_LINEAR

@@ -12,7 +12,8 @@
 // properties, Wall / MovingWall / Inlet / Outlet velocity and FixedGradient
 // / FixedValue pressure patches, Green-Gauss gradients, no momentum source,
 // temperature or buoyancy, and no adaptive relaxation or CPU solver
-// fallback.  Every other call runs the reference's own loop (compiled
+// fallback; rectilinear 2D meshes (createRectilinear2D / createGraded2D) are
+// taken too.  Every other call runs the reference's own loop (compiled
 // beside the shim as ReferenceCpuSIMPLE, simple_reference_bridge.cpp), and
 // the reason the GPU loop was not taken is recorded in
 // gpuDiscretizationFallbackReason, as the reference records its own
@@ -45,6 +46,7 @@
 #include "cfd/core/Exception.hpp"
 #include "cfd/core/Logger.hpp"
 #include "cfd/mesh/MeshGeometry.hpp"
+#include "cfd/mesh/MeshGrading.hpp"
 #include "cfd/pressure_velocity/SIMPLE.hpp"
 #include "cfd/solver/SolverRobustness.hpp"
 #include "cfdb_shim.hpp"
@@ -60,6 +62,61 @@ using cfd::pressure_velocity::SIMPLEStatus;
 
 bool same_vec(const cfd::Vector2& a, const cfd::Vector2& b) {
   return a.x == b.x && a.y == b.y && a.z == b.z;
+}
+
+bool same_mesh(const cfd::mesh::Mesh& ref, const cfd::mesh::Mesh& mesh) {
+  bool same = ref.numberOfCells() == mesh.numberOfCells() &&
+              ref.numberOfFaces() == mesh.numberOfFaces() &&
+              ref.boundaryPatches().size() == mesh.boundaryPatches().size();
+  for (Index c = 0; same && c < mesh.numberOfCells(); ++c)
+    same = same_vec(ref.cell(c).centroid(), mesh.cell(c).centroid()) &&
+           ref.cell(c).volume() == mesh.cell(c).volume();
+  for (Index f = 0; same && f < mesh.numberOfFaces(); ++f) {
+    const cfd::mesh::Face& a = ref.face(f);
+    const cfd::mesh::Face& b = mesh.face(f);
+    same = a.owner() == b.owner() && a.neighbor() == b.neighbor() &&
+           same_vec(a.centroid(), b.centroid()) && same_vec(a.areaVector(), b.areaVector());
+  }
+  for (size_t p = 0; same && p < mesh.boundaryPatches().size(); ++p)
+    same = ref.boundaryPatches()[p].name() == mesh.boundaryPatches()[p].name() &&
+           ref.boundaryPatches()[p].faceIds() == mesh.boundaryPatches()[p].faceIds();
+  return same;
+}
+
+// A 2D structured block whose vertices form a tensor product of two node
+// lists and whose mesh is exactly createRectilinear2D of them
+// (MeshGeometry.cpp:518-555, createGraded2D included); fills the grid and
+// the node coordinates on success.
+bool rectilinear_2d(const cfd::mesh::Mesh& mesh, cfdb_grid* g, std::vector<double> nodes[3],
+                    std::string* why) {
+  const cfd::mesh::StructuredGrid* sg = mesh.structuredGrid();
+  if (!sg || sg->isThreeDimensional() || sg->vertices.size() != (sg->nx + 1) * (sg->ny + 1))
+    return false;
+  const Index nx = sg->nx, ny = sg->ny;
+  std::vector<double> xn(nx + 1), yn(ny + 1);
+  for (Index i = 0; i <= nx; ++i) xn[i] = sg->vertex(i, 0).x;
+  for (Index j = 0; j <= ny; ++j) yn[j] = sg->vertex(0, j).y;
+  for (Index j = 0; j <= ny; ++j)
+    for (Index i = 0; i <= nx; ++i)
+      if (sg->vertex(i, j).x != xn[i] || sg->vertex(i, j).y != yn[j]) return false;
+  try {
+    const cfd::mesh::Mesh ref = cfd::mesh::MeshGeometry::createRectilinear2D(
+        cfd::mesh::AxisSpacing::fromNodes(xn), cfd::mesh::AxisSpacing::fromNodes(yn));
+    if (!same_mesh(ref, mesh)) return false;
+  } catch (const cfd::InvalidArgumentError&) {
+    return false;
+  }
+  g->dim = 2;
+  g->n[0] = static_cast<int64_t>(nx);
+  g->n[1] = static_cast<int64_t>(ny);
+  g->n[2] = 1;
+  g->len[0] = xn[nx] - xn[0];
+  g->len[1] = yn[ny] - yn[0];
+  g->len[2] = 1.0;
+  nodes[0] = std::move(xn);
+  nodes[1] = std::move(yn);
+  (void)why;
+  return true;
 }
 
 // The mesh is exactly createCartesian2D/3D(n..., L...) (same cells, faces,
@@ -95,22 +152,7 @@ bool uniform_cartesian(const cfd::mesh::Mesh& mesh, cfdb_grid* g, std::string* w
   const cfd::mesh::Mesh ref =
       dim == 3 ? cfd::mesh::MeshGeometry::createCartesian3D(n[0], n[1], n[2], len[0], len[1], len[2])
                : cfd::mesh::MeshGeometry::createCartesian2D(n[0], n[1], len[0], len[1]);
-  bool same = ref.numberOfCells() == mesh.numberOfCells() &&
-              ref.numberOfFaces() == mesh.numberOfFaces() &&
-              ref.boundaryPatches().size() == mesh.boundaryPatches().size();
-  for (Index c = 0; same && c < mesh.numberOfCells(); ++c)
-    same = same_vec(ref.cell(c).centroid(), mesh.cell(c).centroid()) &&
-           ref.cell(c).volume() == mesh.cell(c).volume();
-  for (Index f = 0; same && f < mesh.numberOfFaces(); ++f) {
-    const cfd::mesh::Face& a = ref.face(f);
-    const cfd::mesh::Face& b = mesh.face(f);
-    same = a.owner() == b.owner() && a.neighbor() == b.neighbor() &&
-           same_vec(a.centroid(), b.centroid()) && same_vec(a.areaVector(), b.areaVector());
-  }
-  for (size_t p = 0; same && p < mesh.boundaryPatches().size(); ++p)
-    same = ref.boundaryPatches()[p].name() == mesh.boundaryPatches()[p].name() &&
-           ref.boundaryPatches()[p].faceIds() == mesh.boundaryPatches()[p].faceIds();
-  if (!same) {
+  if (!same_mesh(ref, mesh)) {
     *why = "the mesh differs from MeshGeometry::createCartesian" + std::to_string(dim) + "D";
     return false;
   }
@@ -185,6 +227,7 @@ struct Plan {
   cfdb_simple_case cs{};
   cfdb_simple_settings ss{};
   cfdb_simple* session = nullptr;
+  std::vector<double> nodes[3];  // node coordinates of a rectilinear mesh
 };
 
 bool gpu_loop_requested(const SIMPLESettings& s) {
@@ -252,7 +295,14 @@ bool plan_gpu_loop(const SIMPLESettings& settings, Index referenceCell,
     *why = "convection scheme";
     return false;
   }
-  if (!uniform_cartesian(mesh, &plan->cs.grid, why)) return false;
+  std::string uniform_why;
+  if (!uniform_cartesian(mesh, &plan->cs.grid, &uniform_why)) {
+    if (!rectilinear_2d(mesh, &plan->cs.grid, plan->nodes, why)) {
+      *why = uniform_why + ", and it is not a rectilinear 2D mesh either";
+      return false;
+    }
+    for (int a = 0; a < 2; ++a) plan->cs.nodes[a] = plan->nodes[a].data();
+  }
   const int dim = plan->cs.grid.dim;
   if (!boundary_conditions(mesh, dim, vbcs, pbcs, &plan->cs, why)) return false;
   plan->cs.rho = fluid.density();

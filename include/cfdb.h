@@ -280,8 +280,15 @@ enum { CFDB_SCHEME_UPWIND = 0, CFDB_SCHEME_CENTRAL = 1, CFDB_SCHEME_LINEAR_UPWIN
  * RhieChow in 3D (resolveFaceFluxScheme). */
 enum { CFDB_FLUX_LINEAR = 0, CFDB_FLUX_RHIE_CHOW = 1, CFDB_FLUX_AUTOMATIC = 2 };
 
-/* A laminar incompressible case on a uniform Cartesian grid: the mesh of
- * MeshGeometry::createCartesian2D/3D, one BC per patch, constant rho, mu. */
+/* A laminar incompressible case on a Cartesian grid, one BC per patch,
+ * constant rho, mu.  Uniform axes are those of
+ * MeshGeometry::createCartesian2D/3D (spacing len/n); an axis with node
+ * coordinates is that of MeshGeometry::createRectilinear2D / createGraded2D
+ * (MeshGeometry.hpp:228-240, AxisSpacing::fromNodes): nodes[a] holds its
+ * n[a] + 1 strictly increasing node coordinates (host memory, copied at
+ * session creation; len[a] is then not used), NULL for a uniform axis.
+ * Cell centres, widths, face areas and volumes follow from the nodes as the
+ * reference's AxisSpacing computes them. */
 typedef struct {
   cfdb_grid grid;
   int vbc_type[6];
@@ -289,6 +296,7 @@ typedef struct {
   int pbc_type[6];
   double pbc_value[6];
   double rho, mu;
+  const double* nodes[3];
 } cfdb_simple_case;
 
 /* SIMPLESettings (include/cfd/pressure_velocity/SIMPLESettings.hpp:42-145),
@@ -391,7 +399,7 @@ CFDB_API cfdb_status cfdb_simple_write_results(cfdb_simple* s, const double* his
  * (converged or failed) and keeps its state; the others go on.  Per case the
  * stages, statuses and convergence test are those of cfdb_simple_iterate.
  * Supported: FP64 linear solves, CG or BiCGSTAB, no or Jacobi
- * preconditioning (others return CFDB_ERR_UNSUPPORTED). */
+ * preconditioning, uniform grids (others return CFDB_ERR_UNSUPPORTED). */
 typedef struct cfdb_batch cfdb_batch;
 
 /* Launch shapes of the batch: cells (faces) per tile and threads per block
