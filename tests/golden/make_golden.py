@@ -41,6 +41,14 @@ SIMPLE = {
     # Jacobi-CG p' to 1e-8) on a 32^3 cavity, to convergence
     "cavity3d_32_lud_rc_re1000": ("dim=3 nx=32 ny=32 nz=32 mu=0.001 scheme=lud flux=rhiechow "
                                   "outer=5000", ["u", "v", "w", "p", "flux"]),
+    # rectilinear (graded) meshes, createGraded2D with geometric ratios: the
+    # node coordinates are stored with the fields
+    "cavity2d_24_graded": ("dim=2 nx=24 ny=24 gradex=1.12 gradey=1.12 outer=20000",
+                           ["u", "v", "p", "flux"]),
+    "cavity2d_24_graded_lud_rc": ("dim=2 nx=24 ny=20 gradex=1.1 gradey=1.15 cluster=start "
+                                  "scheme=lud flux=rhiechow outer=20000", ["u", "v", "p", "flux"]),
+    "channel2d_32x12_graded": ("dim=2 nx=32 ny=12 lx=6 ly=1 flow=channel mu=0.05 gradey=1.2 "
+                               "outer=300", ["u", "v", "p", "flux"]),
     "cavity3d_8_quick_rc": ("dim=3 nx=8 ny=8 nz=8 mu=0.001 scheme=quick flux=rhiechow outer=40 "
                             "psolver=bicgstab ppre=none prel=1e-4 pabs=1e-13 mrel=1e-6 mabs=1e-13 "
                             "tolu=1e-7 tolp=1e-7 tolc=1e-7", ["u", "v", "w", "p", "flux"]),
@@ -73,6 +81,9 @@ def main(only=()):
             meta = run("simple", args, d)
             arrays = {f: np.fromfile(os.path.join(d, f + ".bin")) for f in fields}
             arrays["hist"] = np.fromfile(os.path.join(d, "hist.bin"))
+            for nd in ("x_nodes", "y_nodes"):  # graded meshes
+                if os.path.exists(os.path.join(d, nd + ".bin")):
+                    arrays[nd] = np.fromfile(os.path.join(d, nd + ".bin"))
             np.savez_compressed(os.path.join(HERE, name + ".npz"), **arrays,
                                 meta=json.dumps({**meta, "args": args}))
             print(name, meta["status"], meta["iterations"])

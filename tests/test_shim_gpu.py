@@ -88,7 +88,8 @@ def test_plugin_momentum_and_pressure_solves_under_the_reference_loop():
 
 
 @pytest.mark.parametrize("name", ["cavity2d_129_config1", "cavity2d_16_lud",
-                                  "channel2d_32x8_central_rc", "cavity3d_8_quick_rc"])
+                                  "channel2d_32x8_central_rc", "cavity3d_8_quick_rc",
+                                  "cavity2d_24_graded_lud_rc", "channel2d_32x12_graded"])
 def test_gpu_outer_loop_through_the_reference_simple_api(name):
     """Both backends GPU: SIMPLE::solve runs the GPU loop (configuration 1 at
     129^2 included) and lands on the reference's fields."""

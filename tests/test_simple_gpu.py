@@ -22,7 +22,10 @@ def _kv(args):
     return dict(a.split("=", 1) for a in args.split())
 
 
-def gpu_case_from_args(args):
+def gpu_case_from_args(args, golden=None):
+    """The case and settings of a reference driver argument string; a graded
+    mesh (gradex / gradey) takes the reference's node coordinates from the
+    golden fixture."""
     from cfdapp_b200.cfdb import LinearSolverSettings, SIMPLESettings, SimpleCase
     a = _kv(args)
     dim = int(a.get("dim", 2))
@@ -44,6 +47,8 @@ def gpu_case_from_args(args):
                               max_iterations=int(a.get("pmax", 5000)),
                               type=a.get("psolver", "cg"),
                               preconditioner=a.get("ppre", "jacobi"))
+    if "gradex" in a or "gradey" in a:
+        case.nodes = (golden["x_nodes"], golden["y_nodes"])
     s = SIMPLESettings(max_iterations=int(a.get("outer", 1000)),
                        velocity_relaxation=float(a.get("au", 0.7)),
                        pressure_relaxation=float(a.get("ap", 0.3)),
@@ -112,11 +117,14 @@ def _golden(name):
 
 @pytest.mark.parametrize("name", ["cavity2d_20_bicgstab", "cavity2d_16_jacobicg",
                                   "channel2d_32x8_central_rc", "cavity2d_16_lud",
-                                  "cavity3d_8_quick_rc", "cavity2d_129_config1"])
+                                  "cavity3d_8_quick_rc", "cavity2d_129_config1",
+                                  "cavity3d_32_lud_rc_re1000", "cavity2d_33_jacobicg",
+                                  "cavity2d_24_graded", "cavity2d_24_graded_lud_rc",
+                                  "channel2d_32x12_graded"])
 def test_simple_matches_reference_outputs(ctx, name):
     from cfdapp_b200.cfdb import simple_solve
     g, meta = _golden(name)
-    case, s = gpu_case_from_args(meta["args"])
+    case, s = gpu_case_from_args(meta["args"], g)
     r = simple_solve(ctx, case, s)
     assert r.status == meta["status"]
     if meta["status"] == "Converged":
@@ -151,7 +159,8 @@ def test_simple_failure_statuses(ctx):
 
 @pytest.mark.parametrize("name", ["cavity2d_16_jacobicg", "channel2d_32x8_central_rc",
                                   "cavity2d_16_lud", "cavity3d_8_quick_rc",
-                                  "cavity2d_129_config1"])
+                                  "cavity2d_129_config1", "cavity3d_32_lud_rc_re1000",
+                                  "cavity2d_24_graded"])
 def test_simple_with_learned_pressure_solver_matches_reference(ctx, name):
     """The same SIMPLE runs with every p' system solved by the learned-
     preconditioned FCG (to the same tolerance) land on the reference's fields."""
@@ -159,7 +168,7 @@ def test_simple_with_learned_pressure_solver_matches_reference(ctx, name):
     g, meta = _golden(name)
     args = meta["args"].replace("psolver=bicgstab", "psolver=cg")
     args = " ".join(a for a in args.split() if not a.startswith("ppre="))
-    case, s = gpu_case_from_args(args + " psolver=cg ppre=learned_mg")
+    case, s = gpu_case_from_args(args + " psolver=cg ppre=learned_mg", g)
     r = simple_solve(ctx, case, s)
     assert r.status == meta["status"]
     if meta["status"] == "Converged":
