@@ -79,19 +79,20 @@ def test_refuses_what_is_not_on_the_gpu_path(tmp_path, fn, change):
 def _compare(out_dir, fixture, iterations_bar=0.02, p_rel_tol=1e-8):
     """Fields within 1e-6 relative L2 of the reference's committed run.  A case
     whose own p' solves stop at a looser relative tolerance (the reference's
-    40x40 and 80x80 examples: 1e-6 and 1e-5) leaves its pressure as exact as
-    that stopping point, which follows the solver's rounding: the pressure
-    bar is then 1e-5."""
+    40x40 and 80x80 examples: 1e-6 and 1e-5) leaves its fields as exact as
+    that stopping point, which follows the solver's rounding (measured: p
+    6.7e-6 at 40x40, u 1.3e-6 at 80x80): the bar is then 1e-5."""
     g = np.load(os.path.join(GOLDEN, fixture + ".npz"))
     rows = open(os.path.join(out_dir, "fields.csv")).read().splitlines()
     col = {h: i for i, h in enumerate(rows[0].split(","))}
     f = np.array([[float(x) for x in r.split(",")] for r in rows[1:]])
     rel = lambda a, b: np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
-    assert rel(f[:, col["velocity_x"]], g["u"]) <= 1e-6
-    assert rel(f[:, col["velocity_y"]], g["v"]) <= 1e-6
+    bar = 1e-6 if p_rel_tol <= 1e-8 else 1e-5
+    assert rel(f[:, col["velocity_x"]], g["u"]) <= bar
+    assert rel(f[:, col["velocity_y"]], g["v"]) <= bar
     if "velocity_z" in col:
-        assert rel(f[:, col["velocity_z"]], g["w"]) <= 1e-6
-    assert rel(f[:, col["pressure"]], g["p"]) <= (1e-6 if p_rel_tol <= 1e-8 else 1e-5)
+        assert rel(f[:, col["velocity_z"]], g["w"]) <= bar
+    assert rel(f[:, col["pressure"]], g["p"]) <= bar
     res = open(os.path.join(out_dir, "residuals.csv")).read().splitlines()
     assert abs((len(res) - 1) - len(g["hist"])) <= max(2, iterations_bar * len(g["hist"]))
     assert os.path.exists(os.path.join(out_dir, "solution.vtk"))
