@@ -1013,6 +1013,7 @@ int flat_blocks(int64_t n) {
 }
 
 #include "mg_quad.cuh"
+#include "mg_stage.cuh"
 
 // Launchers of one level's passes, with the cells-per-thread choice.
 template <int DIM, int CX>
@@ -1043,34 +1044,40 @@ struct LevelOps {
   }
 };
 
-// Blocks of `fn` resident on the whole GPU at `threads` threads per block
-// (registers and shared memory permitting), cached per kernel.  A quad pass
-// launched with at most this many blocks runs in one wave.
-int one_wave(const void* fn, int threads) {
+// Blocks of `fn` resident on the whole current GPU at `threads` threads per
+// block and `dyn` bytes of dynamic shared memory (registers and shared
+// memory permitting), cached per kernel and device; a kernel that needs more
+// than the default 48 KB of dynamic shared memory is opted in on the
+// device's first query.  A quad pass launched with at most this many blocks
+// runs in one wave.
+int one_wave(const void* fn, int threads, size_t dyn = 0) {
   static std::mutex mu;  // contexts on other host threads share the cache
-  static std::map<const void*, int> cache;
-  static int sms = 0;
+  static std::map<std::pair<const void*, int>, int> cache;
   std::lock_guard<std::mutex> lock(mu);
-  auto it = cache.find(fn);
-  if (it != cache.end()) return it->second;
-  if (sms == 0) {
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess ||
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1)
-      sms = 148;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
     cudaGetLastError();
+    dev = 0;
   }
+  auto it = cache.find({fn, dev});
+  if (it != cache.end()) return it->second;
+  int sms = 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1) {
+    cudaGetLastError();
+    sms = 148;
+  }
+  if (dyn > 48 * 1024) cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
   int per = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, threads, 0) != cudaSuccess || per < 1) {
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, threads, dyn) != cudaSuccess || per < 1) {
     cudaGetLastError();
     per = 1;
   }
-  return cache[fn] = per * sms;
+  return cache[{fn, dev}] = per * sms;
 }
 
 template <int DIM>
-int quad_wave(const void* fn, const Seg& sg) {
-  return quad_grid<DIM>(sg, one_wave(fn, Quad<DIM>::TX * Quad<DIM>::TY));
+int quad_wave(const void* fn, const Seg& sg, size_t dyn = 0) {
+  return quad_grid<DIM>(sg, one_wave(fn, Quad<DIM>::TX * Quad<DIM>::TY, dyn));
 }
 
 // Answers every quad pass's occupancy query once, before any stream capture.
@@ -1082,12 +1089,13 @@ void warm_quad_waves() {
   quad_wave<2>((const void*)k_sm_q<2, SM_FIRST, false>, sg);
   quad_wave<2>((const void*)k_sm_q<2, SM_ADD, true>, sg);
   quad_wave<2>((const void*)k_sm_q<2, SM_ADD, false>, sg);
-  quad_wave<3>((const void*)k_res_q<3, false, true>, sg);
-  quad_wave<3>((const void*)k_res_q<3, true, false>, sg);
-  quad_wave<3>((const void*)k_res_q<3, false, false>, sg);
-  quad_wave<3>((const void*)k_sm_q<3, SM_FIRST, false>, sg);
-  quad_wave<3>((const void*)k_sm_q<3, SM_ADD, true>, sg);
-  quad_wave<3>((const void*)k_sm_q<3, SM_ADD, false>, sg);
+  quad_wave<3>((const void*)k_res_s<false, true>, sg, res_s_smem());
+  quad_wave<3>((const void*)k_res_s<true, false>, sg, res_s_smem());
+  quad_wave<3>((const void*)k_res_s<false, false>, sg, res_s_smem());
+  quad_wave<3>((const void*)k_sm_s<SM_FIRST, false>, sg, sm_s_smem());
+  quad_wave<3>((const void*)k_sm_s<SM_ADD, true>, sg, sm_s_smem());
+  quad_wave<3>((const void*)k_sm_s<SM_ADD, false>, sg, sm_s_smem());
+  quad_wave<3>((const void*)k_dir_s, sg, dir_s_smem());
 }
 
 template <int DIM>
@@ -1103,6 +1111,20 @@ void level_res(const MgLevel& M, const LV& LC, const float* x, const float* ec, 
     } else {
       launch(k_res_f<DIM, false>, flat_blocks(M.cells), 256, 0, st, L, LC, x, ec, cw, r, res, skip);
     }
+  } else if (DIM == 3 && quad_ok<DIM>(M.n[0])) {
+    const Seg sg = make_quad_seg<3>(M.n[0], M.n[1], M.n[2]);
+    constexpr int T = PlaneTile::T;
+    constexpr size_t SM = res_s_smem();
+    const LV L = lv(M);
+    if (rc)
+      launch(k_res_s<false, true>, quad_wave<3>((const void*)k_res_s<false, true>, sg, SM), T, SM,
+             st, L, LC, sg, x, ec, cw, r, res, rc, skip);
+    else if (ec)
+      launch(k_res_s<true, false>, quad_wave<3>((const void*)k_res_s<true, false>, sg, SM), T, SM,
+             st, L, LC, sg, x, ec, cw, r, res, rc, skip);
+    else
+      launch(k_res_s<false, false>, quad_wave<3>((const void*)k_res_s<false, false>, sg, SM), T, SM,
+             st, L, LC, sg, x, ec, cw, r, res, rc, skip);
   } else if (quad_ok<DIM>(M.n[0])) {
     const Seg sg = make_quad_seg<DIM>(M.n[0], M.n[1], M.n[2]);
     constexpr int T = Quad<DIM>::TX * Quad<DIM>::TY;
@@ -1131,6 +1153,20 @@ void level_sm(const MgLevel& M, const LV& LC, const Kern& K, bool first, const f
       launch(k_sm_f<DIM, SM_FIRST>, flat_blocks(M.cells), 256, 0, st, L, LC, K, src, ec, cw, x, skip, pin, r);
     else
       launch(k_sm_f<DIM, SM_ADD>, flat_blocks(M.cells), 256, 0, st, L, LC, K, src, ec, cw, x, skip, pin, r);
+  } else if (DIM == 3 && quad_ok<DIM>(M.n[0])) {
+    const Seg sg = make_quad_seg<3>(M.n[0], M.n[1], M.n[2]);
+    constexpr int T = PlaneTile::T;
+    constexpr size_t SM = sm_s_smem();
+    const LV L = lv(M);
+    if (first)
+      launch(k_sm_s<SM_FIRST, false>, quad_wave<3>((const void*)k_sm_s<SM_FIRST, false>, sg, SM), T,
+             SM, st, L, LC, sg, K, src, ec, cw, x, skip, pin, r, Hook{});
+    else if (hook)
+      launch(k_sm_s<SM_ADD, true>, quad_wave<3>((const void*)k_sm_s<SM_ADD, true>, sg, SM), T, SM, st,
+             L, LC, sg, K, src, ec, cw, x, skip, pin, r, *hook);
+    else
+      launch(k_sm_s<SM_ADD, false>, quad_wave<3>((const void*)k_sm_s<SM_ADD, false>, sg, SM), T, SM,
+             st, L, LC, sg, K, src, ec, cw, x, skip, pin, r, Hook{});
   } else if (quad_ok<DIM>(M.n[0])) {
     const Seg sg = make_quad_seg<DIM>(M.n[0], M.n[1], M.n[2]);
     constexpr int T = Quad<DIM>::TX * Quad<DIM>::TY;
@@ -1557,14 +1593,21 @@ void launch_dir_q(LearnedSolver* s, const FineOperator& op, Loop h, cudaStream_t
          s->p0, s->p1, s->q, s->r, s->partials, h);
 }
 
+void launch_dir_s(LearnedSolver* s, const FineOperator& op, Loop h, cudaStream_t st) {
+  const Seg sg = make_quad_seg<3>(op.A.nx, op.A.ny, op.A.nz);
+  constexpr size_t SM = dir_s_smem();
+  const int grid = quad_wave<3>((const void*)k_dir_s, sg, SM);
+  launch(k_dir_s, grid, PlaneTile::T, SM, st, op.A, sg, s->S, s->z32, s->p0, s->p1, s->q, s->r,
+         s->partials, h);
+}
+
 void launch_dir(LearnedSolver* s, const FineOperator& op, Loop h, cudaStream_t st) {
   if (op.dim == 2) {
     if (quad_ok<2>(op.A.nx)) launch_dir_q<2>(s, op, h, st);
     else launch_dir_t<2, 1>(s, op, h, st);
   } else {
-    // 3D: the plain pass (measured 4.5 % faster per FCG iteration at 256^3
-    // than the marching one, which stays the faster in 2D)
-    if (quad_ok<3>(op.A.nx)) launch_dir_v<3>(s, op, h, st);
+    // 3D: the staged pass
+    if (quad_ok<3>(op.A.nx)) launch_dir_s(s, op, h, st);
     else launch_dir_t<3, 1>(s, op, h, st);
   }
 }
