@@ -510,6 +510,17 @@ enum { SM_FIRST = 0, SM_ADD = 1 };
 #define CFDB_PDL 1
 #endif
 
+// The first launch error on this host thread since the last take_launch_error()
+// (a launch refused inside a stream capture leaves no node; the capture then
+// reports it instead of instantiating an incomplete graph).
+thread_local cudaError_t g_launch_error = cudaSuccess;
+
+cudaError_t take_launch_error() {
+  const cudaError_t e = g_launch_error;
+  g_launch_error = cudaSuccess;
+  return e;
+}
+
 template <typename... KArgs, typename... Args>
 void launch(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
             Args&&... args) {
@@ -523,7 +534,8 @@ void launch(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaSt
   at[0].val.programmaticStreamSerializationAllowed = CFDB_PDL;
   cfg.attrs = at;
   cfg.numAttrs = 1;
-  cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+  const cudaError_t e = cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+  if (e != cudaSuccess && g_launch_error == cudaSuccess) g_launch_error = e;
 }
 
 // x <- [x] (+ cw P ec) + D^-1/2 (W * (D^-1/2 u)), u = res (SM_ADD) or r with
@@ -1046,10 +1058,11 @@ struct LevelOps {
 
 // Blocks of `fn` resident on the whole current GPU at `threads` threads per
 // block and `dyn` bytes of dynamic shared memory (registers and shared
-// memory permitting), cached per kernel and device; a kernel that needs more
-// than the default 48 KB of dynamic shared memory is opted in on the
-// device's first query.  A quad pass launched with at most this many blocks
-// runs in one wave.
+// memory permitting), cached per kernel and device.  A kernel that takes
+// dynamic shared memory is opted in to `dyn` bytes on the device's first
+// query (without it, static plus dynamic shared memory above 48 KB fails the
+// launch).  A quad pass launched with at most this many blocks runs in one
+// wave.
 int one_wave(const void* fn, int threads, size_t dyn = 0) {
   static std::mutex mu;  // contexts on other host threads share the cache
   static std::map<std::pair<const void*, int>, int> cache;
@@ -1066,7 +1079,7 @@ int one_wave(const void* fn, int threads, size_t dyn = 0) {
     cudaGetLastError();
     sms = 148;
   }
-  if (dyn > 48 * 1024) cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+  if (dyn > 0) cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
   int per = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, threads, dyn) != cudaSuccess || per < 1) {
     cudaGetLastError();
@@ -1648,12 +1661,14 @@ cfdb_status capture_graph(cfdb_context* ctx, LearnedSolver* s, const FineOperato
   cudaGraphConditionalHandle h;
   CFDB_CUDA(ctx, cudaGraphConditionalHandleCreate(&h, s->graph, 1, cudaGraphCondAssignDefault));
   // parent graph: the initial residual, then the WHILE node
+  take_launch_error();
   CFDB_CUDA(ctx, cudaStreamBeginCaptureToGraph(s->cap, s->graph, nullptr, nullptr, 0,
                                                cudaStreamCaptureModeThreadLocal));
   const Loop lp{h, 1};
   launch_init(s, op, lp, s->cap);
   cudaGraph_t g = nullptr;
   cudaError_t ce = cudaStreamEndCapture(s->cap, &g);
+  if (ce == cudaSuccess) ce = take_launch_error();
   if (ce != cudaSuccess) return cuda_error(ctx, ce, "capture of the FCG start", __FILE__, __LINE__);
   size_t nn = 0;
   CFDB_CUDA(ctx, cudaGraphGetNodes(s->graph, nullptr, &nn));
@@ -1673,6 +1688,7 @@ cfdb_status capture_graph(cfdb_context* ctx, LearnedSolver* s, const FineOperato
   const int nv = enqueue_body(s, op, lp, s->cap);
   cudaGraph_t b2 = nullptr;
   ce = cudaStreamEndCapture(s->cap, &b2);
+  if (ce == cudaSuccess) ce = take_launch_error();
   if (ce != cudaSuccess) return cuda_error(ctx, ce, "capture of the FCG loop", __FILE__, __LINE__);
   CFDB_CHECK_LAUNCH(ctx);
   CFDB_CUDA(ctx, cudaGraphInstantiate(&s->exec, s->graph, 0));
