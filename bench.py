@@ -50,8 +50,8 @@ def parse():
                          "iterations of the 256^3 Re-1000 lid-driven cavity")
     ap.add_argument("--n3d", type=int, default=256)
     ap.add_argument("--converge", type=int, default=0,
-                    help="cavity3d: run up to this many outer iterations from rest, to the "
-                         "case's convergence test, instead of timing a few")
+                    help="cavity3d / batched: run up to this many outer iterations from rest, "
+                         "to the cases' convergence test, instead of timing a few")
     ap.add_argument("--history-out", default=None)
     ap.add_argument("--cases", type=int, default=64)
     ap.add_argument("--no-config1", action="store_true",
@@ -64,7 +64,8 @@ def parse():
     ap.add_argument("--n", type=int, default=2048)
     ap.add_argument("--preconditioner", default="learned_mg",
                     choices=["learned_mg", "jacobi", "none"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32_refined"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32_refined"],
+                    help="p' precision of --profile-solve and of the batched workload")
     ap.add_argument("--max-iterations", type=int, default=100000)
     return ap.parse_args()
 
@@ -344,7 +345,7 @@ def batched_cases(seed, ncases):
     return out
 
 
-def batched_settings():
+def batched_settings(precision="fp64"):
     from cfdapp_b200.cfdb import LinearSolverSettings, SIMPLESettings
     return SIMPLESettings(
         max_iterations=100000, velocity_relaxation=0.7, pressure_relaxation=0.3,
@@ -355,7 +356,7 @@ def batched_settings():
                                              max_iterations=500),
         pressure_solver=LinearSolverSettings(type="cg", preconditioner="jacobi",
                                              absolute_tolerance=0.0, relative_tolerance=1e-8,
-                                             max_iterations=20000))
+                                             max_iterations=20000, precision=precision))
 
 
 def batched_cpu_baseline(cases, outer=2):
@@ -391,6 +392,41 @@ def batched_cpu_baseline(cases, outer=2):
             "kind": "reference", "sample": "; ".join(picked)}
 
 
+def run_batched_to_convergence(a, ctx, b, cases, cells, s):
+    """The whole batch from rest until every case has met its convergence
+    test (continuity, velocity and pressure residuals 1e-6) or --converge
+    outer iterations: per-case status and iterations, and the device time."""
+    t0 = time.perf_counter()
+    done = 0
+    dev_ms = 0.0
+    while done < a.converge:
+        step = min(500, a.converge - done)
+        st = b.iterate(step)
+        dev_ms += st["device_ms"]
+        done += step
+        if st["active"] == 0:
+            break
+    res = b.results()
+    statuses = {}
+    for r in res:
+        statuses[r["status"]] = statuses.get(r["status"], 0) + 1
+    its = np.array([r["iterations"] for r in res])
+    line = {"metric": "batched SIMPLE run to convergence", "cases": len(cases),
+            "pressure_precision": a.precision, "statuses": statuses,
+            "outer_iterations": {"min": int(its.min()), "median": float(np.median(its)),
+                                 "max": int(its.max())},
+            "pressure_linear_iterations": int(sum(r["pressure_linear_iterations"] for r in res)),
+            "max_final_continuity": float(max(r["final"]["continuity"] for r in res)),
+            "device_s": dev_ms * 1e-3, "wall_s": time.perf_counter() - t0,
+            "cells": int(cells.sum()),
+            "cases_detail": [{"side": c[1], "kind": c[0], "re": round(c[2], 1),
+                              "status": r["status"], "iterations": r["iterations"]}
+                             for c, r in zip(cases, res)]}
+    print(json.dumps(line), flush=True)
+    b.close()
+    ctx.close()
+
+
 def run_batched(a):
     from cfdapp_b200 import cfdb
     rank, world, local = dist_info()
@@ -405,11 +441,13 @@ def run_batched(a):
         raise SystemExit("bench.py: no sm_100 device visible (the product has no CPU path)")
     ctx = cfdb.Context(local)
     cases = batched_cases(SEED + rank, a.cases)
-    s = batched_settings()
+    s = batched_settings(a.precision)
     b = cfdb.Batch(ctx, [c[3] for c in cases], s)
     for k in range(len(cases)):
         b.set_state(k)
     cells = np.array([c[3].cells() for c in cases], dtype=np.float64)
+    if a.converge > 0:
+        return run_batched_to_convergence(a, ctx, b, cases, cells, s)
 
     def counters():
         r = b.results()

@@ -62,6 +62,7 @@ struct KArgs {
   int mode;  // 0: momentum component `comp`; 1: p'
   int comp;
   int krylov, jacobi;
+  int mixed;  // 1: p' by the mixed-precision CG (CFDB_PRECISION_FP32_REFINED)
   double abs_tol, rel_tol;
   int64_t max_it;
   unsigned* bar;    // 2 words per case
@@ -144,7 +145,26 @@ __global__ void __launch_bounds__(krylov::kThreads, 5) k_batch_krylov(KArgs A) {
     T.s.timeout_ns = kTeamTimeoutNs;
     T.r = rank;
     T.n = n;
-    krylov::krylov_run(P, T);
+    if (A.mixed) {
+      // FP32 storage inside the case's own BiCGSTAB-only vectors (unused by
+      // CG) and the upper halves of p and v: 2 floats per double slot
+      float* w[5] = {reinterpret_cast<float*>(B.krh + o), reinterpret_cast<float*>(B.ks + o),
+                     reinterpret_cast<float*>(B.kt + o), reinterpret_cast<float*>(B.kp + o),
+                     reinterpret_cast<float*>(B.kv + o)};
+      const int64_t nc = K.G.nc;
+      P.m32[0] = w[0];
+      P.m32[1] = w[0] + nc;
+      P.m32[2] = w[1];
+      P.m32[3] = w[1] + nc;
+      P.m32[4] = w[2];
+      P.m32[5] = w[2] + nc;
+      P.m32[6] = w[3] + nc;
+      P.p32 = w[3];
+      P.v32 = w[4];
+      krylov::cg_mixed_run(P, T);
+    } else {
+      krylov::krylov_run(P, T);
+    }
   }
   if (!leader || !A.record) return;
   const int st = (int)out[krylov::O_STATUS];
@@ -305,6 +325,7 @@ void launch_krylov(cfdb_batch* b, int mode, int comp, int record, cudaStream_t s
   A.comp = comp;
   A.krylov = L.krylov;
   A.jacobi = L.preconditioner == CFDB_PRECOND_JACOBI;
+  A.mixed = mode == 1 && L.precision == CFDB_PRECISION_FP32_REFINED;
   A.abs_tol = L.abs_tol;
   A.rel_tol = L.rel_tol;
   A.max_it = L.max_iterations;
@@ -560,11 +581,15 @@ cfdb_status cfdb_batch_create(cfdb_context* ctx, int ncases, const cfdb_simple_c
       st->momentum.max_iterations < 1 || st->pressure.max_iterations < 1)
     return set_error(ctx, CFDB_ERR_INVALID_ARGUMENT, "invalid relaxation or iteration limits");
   for (const cfdb_linear_settings* L : {&st->momentum, &st->pressure}) {
-    if (L->precision != CFDB_PRECISION_FP64 ||
-        (L->preconditioner != CFDB_PRECOND_NONE && L->preconditioner != CFDB_PRECOND_JACOBI) ||
+    if ((L->preconditioner != CFDB_PRECOND_NONE && L->preconditioner != CFDB_PRECOND_JACOBI) ||
         (L->krylov != CFDB_KRYLOV_CG && L->krylov != CFDB_KRYLOV_BICGSTAB))
       return set_error(ctx, CFDB_ERR_UNSUPPORTED,
-                       "batched solves support FP64 CG/BiCGSTAB with no or Jacobi preconditioning");
+                       "batched solves support CG/BiCGSTAB with no or Jacobi preconditioning");
+    const bool mixed_pp = L == &st->pressure && L->krylov == CFDB_KRYLOV_CG &&
+                          L->precision == CFDB_PRECISION_FP32_REFINED;
+    if (L->precision != CFDB_PRECISION_FP64 && !mixed_pp)
+      return set_error(ctx, CFDB_ERR_UNSUPPORTED,
+                       "batched solves take FP64, or FP32_REFINED for a CG p' solve");
   }
   CFDB_CUDA(ctx, cudaSetDevice(ctx->device));
   std::unique_ptr<cfdb_batch> b(new cfdb_batch());

@@ -26,7 +26,7 @@ namespace krylov {
 
 constexpr int kThreads = 256;  // threads per block of every team
 
-enum { O_STATUS = 0, O_ITER = 1, O_B0 = 2, O_FINAL = 3, O_RESTARTS = 4 };
+enum { O_STATUS = 0, O_ITER = 1, O_B0 = 2, O_FINAL = 3, O_RESTARTS = 4, O_REPLACEMENTS = 5 };
 
 struct SParams {
   StencilMatrix M;
@@ -41,6 +41,11 @@ struct SParams {
   int64_t hist_cap;
   double* partials;
   double* out;
+  // mixed-precision CG (cg_mixed_run): the FP32 copies of the diagonal and
+  // the six couplings, the FP32 direction and its product (the caller's
+  // storage, filled by the solve)
+  float* m32[7];
+  float *p32, *v32;
 };
 
 __device__ __forceinline__ double spmv_row(const StencilMatrix& M, const double* v, int64_t c,
@@ -359,6 +364,156 @@ __device__ void krylov_run(const SParams& P, const Team& T) {
     rhoTerms = tot[2];
   }
   finish(CFDB_SOLVER_MAX_ITERATIONS, completed, lastHist);
+}
+
+// The FP32 product of the FP32 copy of the matrix with v (same column order
+// as spmv_row).
+__device__ __forceinline__ float spmv_row32(const StencilMatrix& M, float* const (&m)[7],
+                                            const float* v, int64_t c, int i, int j, int k) {
+  float sum = 0.f;
+  if (M.dim == 3 && k > 0) sum += m[5][c] * __ldcg(v + c - M.sz);
+  if (j > 0) sum += m[3][c] * __ldcg(v + c - M.sy);
+  if (i > 0) sum += m[1][c] * __ldcg(v + c - 1);
+  sum += m[0][c] * __ldcg(v + c);
+  if (i < M.nx - 1) sum += m[2][c] * __ldcg(v + c + 1);
+  if (j < M.ny - 1) sum += m[4][c] * __ldcg(v + c + M.sy);
+  if (M.dim == 3 && k < M.nz - 1) sum += m[6][c] * __ldcg(v + c + M.sz);
+  return sum;
+}
+
+// Mixed-precision CG (+ Jacobi) that keeps one Krylov space: the matrix is
+// copied to FP32 once per solve; the direction p and q = A p live in FP32
+// and the inner product A p runs on the FP32 copy, while x, r and every
+// reduction stay FP64.  The recurrence residual is replaced by the FP64 true
+// residual b - A x (the "reliable updates" of van der Vorst and Ye, 2000)
+// after every ten-fold drop since the last replacement, whenever the
+// recurrence meets the tolerance, and at the iteration cap, so the solve
+// only stops as converged on an FP64 true residual.  Breakdown and
+// non-finite tests are those of the FP64 CG above.
+template <class Team>
+__device__ void cg_mixed_run(const SParams& P, const Team& T) {
+  __shared__ double red[3 * 32];
+  const StencilMatrix& M = P.M;
+  const int B = T.size(), blk = T.rank(), tid = threadIdx.x;
+  const bool leader = (blk == 0 && tid == 0);
+  const int64_t n = M.n;
+  const int64_t c0 = n * blk / B, c1 = n * (blk + 1) / B;
+  int round = 0;
+  auto part = [&]() { return P.partials + (size_t)(round & 1) * 3 * B; };
+  auto coords = [&](int64_t c, int& i, int& j, int& k) {
+    i = (int)(c % M.nx);
+    j = (int)((c / M.nx) % M.ny);
+    k = (int)(c / M.sz);
+  };
+  const double* inv = M.inv;
+  float* const m[7] = {P.m32[0], P.m32[1], P.m32[2], P.m32[3], P.m32[4], P.m32[5], P.m32[6]};
+  float* const p32 = P.p32;
+  float* const v32 = P.v32;
+  auto reduce3 = [&](double a0, double a1, double a2, double (&o)[3]) -> bool {
+    double a[3] = {a0, a1, a2};
+    block_sum<3>(a, red);
+    if (tid == 0) {
+      part()[3 * blk] = a[0];
+      part()[3 * blk + 1] = a[1];
+      part()[3 * blk + 2] = a[2];
+    }
+    if (!T.sync()) return false;
+    grid_total<3>(part(), 3, B, o, red);
+    ++round;
+    return true;
+  };
+  auto finish = [&](int status, int64_t it, double fin, int64_t reps) {
+    if (leader) {
+      P.out[O_STATUS] = status;
+      P.out[O_ITER] = (double)it;
+      P.out[O_FINAL] = fin;
+      P.out[O_REPLACEMENTS] = (double)reps;
+    }
+  };
+  // FP64 true residual r = b - A x; returns (r.r, r.z) through the team
+  auto true_residual = [&](double (&o)[3]) -> bool {
+    double a0 = 0.0, a1 = 0.0;
+    for (int64_t c = c0 + tid; c < c1; c += kThreads) {
+      int i, j, k;
+      coords(c, i, j, k);
+      const double rn = __ldg(P.b + c) - spmv_row(M, P.x, c, i, j, k);
+      P.r[c] = rn;
+      a0 += rn * rn;
+      a1 += rn * (inv ? __ldg(inv + c) * rn : rn);
+    }
+    return reduce3(a0, a1, 0.0, o);
+  };
+
+  // ---- the FP32 copy of the matrix (published to the team by the first
+  // reduction's barrier), then r = b - A x
+  for (int64_t c = c0 + tid; c < c1; c += kThreads) {
+    m[0][c] = (float)__ldg(M.diag + c);
+#pragma unroll
+    for (int q = 0; q < 6; ++q)
+      if (q < 2 * M.dim) m[1 + q][c] = (float)__ldg(M.off[q] + c);
+  }
+  double tot[3];
+  if (!true_residual(tot)) return;
+  const double b0 = sqrt(tot[0]);
+  if (leader) {
+    P.out[O_B0] = b0;
+    P.out[O_RESTARTS] = 0;
+    if (P.hist_cap > 0) P.hist[0] = b0;
+  }
+  auto conv = [&](double res) {
+    return (res <= P.abs_tol) || ((b0 > 0.0) && (res / b0 <= P.rel_tol));
+  };
+  if (b0 == 0.0 || conv(b0)) return finish(CFDB_SOLVER_CONVERGED, 0, b0, 0);
+  double rz = tot[1];
+  if (!isfinite(rz)) return finish(CFDB_SOLVER_BREAKDOWN, 0, b0, 0);
+  double res_cur = b0, res_rep = b0, beta = 0.0;
+  int64_t reps = 0;
+  for (int64_t it = 1; it <= P.max_it; ++it) {
+    // p = z + beta p (FP32), z = M^-1 r rounded to FP32
+    const float bf = (float)beta;
+    for (int64_t c = c0 + tid; c < c1; c += kThreads) {
+      const float z = (float)(inv ? __ldg(inv + c) * __ldcg(P.r + c) : __ldcg(P.r + c));
+      p32[c] = (it == 1) ? z : fmaf(bf, __ldcg(p32 + c), z);
+    }
+    if (!T.sync()) return;
+    double pap = 0.0;
+    for (int64_t c = c0 + tid; c < c1; c += kThreads) {
+      int i, j, k;
+      coords(c, i, j, k);
+      const float ap = spmv_row32(M, m, p32, c, i, j, k);
+      v32[c] = ap;
+      pap += (double)__ldcg(p32 + c) * (double)ap;
+    }
+    if (!reduce3(pap, 0.0, 0.0, tot)) return;
+    const double pAp = tot[0];
+    const double alpha = rz / pAp;
+    if (!isfinite(pAp) || fabs(pAp) < 1.0e-30 || !isfinite(alpha))
+      return finish(CFDB_SOLVER_BREAKDOWN, it - 1, res_cur, reps);
+    double rr = 0.0, rzn = 0.0;
+    for (int64_t c = c0 + tid; c < c1; c += kThreads) {
+      P.x[c] = fma(alpha, (double)__ldcg(p32 + c), P.x[c]);
+      const double rn = fma(-alpha, (double)__ldcg(v32 + c), __ldcg(P.r + c));
+      P.r[c] = rn;
+      rr += rn * rn;
+      rzn += rn * (inv ? __ldg(inv + c) * rn : rn);
+    }
+    if (!reduce3(rr, rzn, 0.0, tot)) return;
+    double res = sqrt(tot[0]);
+    if (isfinite(res) && (conv(res) || res <= 0.1 * res_rep || it == P.max_it)) {
+      if (!true_residual(tot)) return;
+      res = sqrt(tot[0]);
+      res_rep = res;
+      ++reps;
+    }
+    if (leader && it < P.hist_cap) P.hist[it] = res;
+    if (!isfinite(res)) return finish(CFDB_SOLVER_NONFINITE_RESIDUAL, it, res, reps);
+    res_cur = res;
+    if (conv(res)) return finish(CFDB_SOLVER_CONVERGED, it, res, reps);
+    beta = tot[1] / rz;
+    if (!isfinite(tot[1]) || !isfinite(beta)) return finish(CFDB_SOLVER_BREAKDOWN, it, res, reps);
+    rz = tot[1];
+  }
+  return finish(CFDB_SOLVER_MAX_ITERATIONS, P.max_it, res_cur, reps);
 }
 
 }  // namespace krylov

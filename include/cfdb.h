@@ -398,8 +398,13 @@ CFDB_API cfdb_status cfdb_simple_write_results(cfdb_simple* s, const double* his
  * the whole batch is one CUDA graph launch.  Each case stops on its own
  * (converged or failed) and keeps its state; the others go on.  Per case the
  * stages, statuses and convergence test are those of cfdb_simple_iterate.
- * Supported: FP64 linear solves, CG or BiCGSTAB, no or Jacobi
- * preconditioning, uniform grids (others return CFDB_ERR_UNSUPPORTED). */
+ * Supported: CG or BiCGSTAB, no or Jacobi preconditioning, FP64 solves or,
+ * for a CG p' solve, CFDB_PRECISION_FP32_REFINED (a mixed-precision CG that
+ * keeps one Krylov space: FP32 matrix copy, direction and A p; FP64 x, r and
+ * reductions; the FP64 true residual replaces the recurrence after every
+ * ten-fold drop, at the tolerance and at the cap; inner_rel_tol and
+ * max_refinements are not used), uniform grids (others return
+ * CFDB_ERR_UNSUPPORTED). */
 typedef struct cfdb_batch cfdb_batch;
 
 /* Launch shapes of the batch: cells (faces) per tile and threads per block

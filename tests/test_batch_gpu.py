@@ -213,3 +213,33 @@ def test_batch_edge_cases(ctx):
         type="cg", preconditioner="learned_mg"))
     with pytest.raises(CfdbError):
         Batch(ctx, [SimpleCase.cavity(2, 8)], learned)
+
+
+@pytest.mark.parametrize("name", ["cavity2d_16_jacobicg", "cavity3d_32_lud_rc_re1000"])
+def test_batch_mixed_precision_pprime_matches_reference(ctx, name):
+    """The batch's FP32_REFINED p' solve (a mixed-precision CG that keeps one
+    Krylov space, FP64 residual replacement): every p' solve still stops on
+    an FP64 true residual at the case's tolerance, so the golden case lands
+    on the reference's fields with the single-case bar (outer iterations
+    within 2 %, fields within 1e-6 relative L2)."""
+    from cfdapp_b200.cfdb import Batch
+    import dataclasses
+    g, meta = _golden(name)
+    case, s = gpu_case_from_args(meta["args"])
+    s = dataclasses.replace(s, pressure_solver=dataclasses.replace(s.pressure_solver,
+                                                                  precision="fp32_refined"))
+    other = gpu_case_from_args(_extras(meta["args"])[0])[0]
+    b = Batch(ctx, [other, case], s)
+    for k in range(2):
+        b.set_state(k)
+    b.iterate(s.max_iterations)
+    r = b.results()[1]
+    assert r["status"] == meta["status"] == "Converged"
+    assert abs(r["iterations"] - meta["iterations"]) <= max(2, 0.02 * meta["iterations"])
+    u, v, w, p, f = b.get_state(1)
+    for fld, arr in (("u", u), ("v", v), ("w", w), ("p", p)):
+        if fld in g.files:
+            assert _rel(arr, g[fld]) <= 1e-6, fld
+    assert _rel(f, g["flux"]) <= 1e-6
+    assert b.results()[0]["status"] == "Converged"
+    b.close()
