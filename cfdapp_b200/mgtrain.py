@@ -235,17 +235,38 @@ def fcg_iterations(ctx, ops, b_list):
     return its
 
 
-def train_dim(ctx, dim, steps, seed, log, hard, nu=2, sweeps=50):
+def train_dim(ctx, dim, steps, seed, log, hard, nu=2, sweeps=50, grids=None, re_samples=0,
+              val_n=None):
+    """grids=None: the compact recipe (one 128^2 / 32^3 grid, cavities at Re
+    100, 400, 1000).  grids=[n, ...]: p' systems harvested from cavity runs on
+    every grid n^dim at `re_samples` Reynolds numbers drawn uniformly from
+    [100, 1000] each (one snapshot after 20-100 outer iterations), plus the
+    isolated and two smooth-response operators on the first grid."""
     rng = np.random.default_rng(seed)
     n_train = (128, 128) if dim == 2 else (32, 32, 32)
     n_val = (384, 384) if dim == 2 else (64, 64, 64)
+    if val_n:
+        n_val = (val_n,) * dim
     # training operators: isolated, smooth random response, and p' systems
     # harvested from the solver's own SIMPLE runs of cavities at Re 100..1000
-    train_fc = [uniform_faces(dim, n_train)] + [random_operator_faces(dim, n_train, rng)
-                                                for _ in range(2)]
-    harvested = harvest_cavity(ctx, dim, n_train[0], [100.0, 400.0, 1000.0], 2)
-    train_fc += [f for f, _, _ in harvested]
-    train_ops = [cfdb.POperator(ctx, dim, n_train, face_coeff=fc) for fc in train_fc]
+    if grids:
+        n_train = (grids[0],) * dim
+    train_set = [(n_train, uniform_faces(dim, n_train))] + \
+        [(n_train, random_operator_faces(dim, n_train, rng)) for _ in range(2)]
+    if grids:
+        harvested = []
+        for g in grids:
+            for re in rng.uniform(100.0, 1000.0, size=re_samples):
+                h = harvest_cavity(ctx, dim, g, [float(re)], 1, chunk=int(rng.integers(20, 101)))
+                harvested += [((g,) * dim, f) for f, _, _ in h]
+                log(f"dim {dim}: harvested {g}^{dim} at Re {re:.0f}")
+    else:
+        harvested = [(n_train, f) for f, _, _ in
+                     harvest_cavity(ctx, dim, n_train[0], [100.0, 400.0, 1000.0], 2)]
+    train_set += harvested
+    train_fc = [fc for _, fc in train_set]
+    train_sz = [sz for sz, _ in train_set]
+    train_ops = [cfdb.POperator(ctx, dim, sz, face_coeff=fc) for sz, fc in train_set]
     log(f"dim {dim}: {len(train_ops)} training operators ({len(harvested)} harvested)")
     # validation: the isolated system, a smooth-response system and a
     # harvested cavity system (Re 700), synthetic RHS
@@ -272,9 +293,9 @@ def train_dim(ctx, dim, steps, seed, log, hard, nu=2, sweeps=50):
     for step in range(1, steps + 1):
         q = step % len(train_ops)
         op = train_ops[q]
-        e = multiscale_errors(dim, n_train, 4, rng)
+        e = multiscale_errors(dim, train_sz[q], 4, rng)
         if hard:
-            e[4 - hard:] = hard_errors(op, dim, n_train, train_fc[q], e[4 - hard:])
+            e[4 - hard:] = hard_errors(op, dim, train_sz[q], train_fc[q], e[4 - hard:])
         loss, gk, gc = op.mg_loss_grad(e)
         lr = lr0 * 0.5 * (1.0 + np.cos(np.pi * step / steps))
         g = P.grad_vector(gk, gc)
@@ -295,6 +316,8 @@ def train_dim(ctx, dim, steps, seed, log, hard, nu=2, sweeps=50):
     return P, {"untrained_validation_iterations": untrained,
                "trained_validation_iterations": best[2],
                "validation_grids": list(n_val), "training_grid": list(n_train),
+               "training_grids": sorted({int(sz[0]) for sz in train_sz}),
+               "harvested_systems": len(harvested),
                "loss_first50": float(np.mean(history[:50])),
                "loss_last50": float(np.mean(history[-50:])), "steps": steps,
                "nu": nu, "coarse_sweeps": sweeps, "hard_samples_of_4": hard}
@@ -360,6 +383,13 @@ def main():
                     help="damped-Jacobi sweeps on the coarsest level, per dim (2D, 3D)")
     ap.add_argument("--hard", type=int, nargs="+", default=[0, 2],
                     help="per dim (2D, 3D): samples of 4 drawn by power iteration of I - M A")
+    ap.add_argument("--grids2d", type=int, nargs="*", default=None,
+                    help="2D: harvest p' systems on these grids (e.g. 256 512 1024) at "
+                         "--re-samples Reynolds numbers uniform in [100, 1000] each")
+    ap.add_argument("--re-samples", type=int, default=2)
+    ap.add_argument("--val2d", type=int, default=None, help="2D validation grid (default 384)")
+    ap.add_argument("--keep", default=None,
+                    help="mg_weights.json whose sets for the dimensions not trained are kept")
     ap.add_argument("--out", default=os.path.join(os.path.dirname(__file__), "csrc"))
     a = ap.parse_args()
     ctx = cfdb.Context(0)
@@ -370,7 +400,16 @@ def main():
         q = 0 if dim == 2 else 1
         pick = lambda v: v[q] if len(v) > q else v[-1]
         sets[dim] = train_dim(ctx, dim, a.steps, a.seed + dim, log, pick(a.hard), pick(a.nu),
-                              pick(a.coarse_sweeps))
+                              pick(a.coarse_sweeps), grids=a.grids2d if dim == 2 else None,
+                              re_samples=a.re_samples, val_n=a.val2d if dim == 2 else None)
+    if a.keep:
+        with open(a.keep) as f:
+            old_sets = json.load(f)["sets"]
+        for d, rec in old_sets.items():
+            if int(d) not in sets:
+                P = Params(int(d), rec["kernels"], rec["coarse_weights"])
+                sets[int(d)] = (P, dict(rec["record"], nu=rec["nu"],
+                                        coarse_sweeps=rec["coarse_sweeps"]))
     digest = write_outputs(a.out, sets)
     log(f"wrote {a.out}/mg_trained.inc and mg_weights.json (sha256 {digest[:16]})")
     ctx.close()
