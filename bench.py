@@ -404,6 +404,8 @@ def run_batched_to_convergence(a, ctx, b, cases, cells, s):
         st = b.iterate(step)
         dev_ms += st["device_ms"]
         done += step
+        print(json.dumps({"outer": done, "active": st["active"], "device_s": dev_ms * 1e-3}),
+              file=sys.stderr, flush=True)
         if st["active"] == 0:
             break
     res = b.results()
