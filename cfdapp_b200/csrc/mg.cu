@@ -1108,7 +1108,8 @@ void warm_quad_waves() {
   quad_wave<3>((const void*)k_sm_s<SM_FIRST, false>, sg, sm_s_smem());
   quad_wave<3>((const void*)k_sm_s<SM_ADD, true>, sg, sm_s_smem());
   quad_wave<3>((const void*)k_sm_s<SM_ADD, false>, sg, sm_s_smem());
-  quad_wave<3>((const void*)k_dir_s, sg, dir_s_smem());
+  quad_wave<3>((const void*)k_dir_s<true>, sg, dir_s_smem());
+  quad_wave<3>((const void*)k_dir_s<false>, sg, dir_s_smem());
 }
 
 template <int DIM>
@@ -1601,6 +1602,12 @@ template <int DIM>
 template <int DIM>
 void launch_dir_q(LearnedSolver* s, const FineOperator& op, Loop h, cudaStream_t st) {
   const Seg sg = make_quad_seg<DIM>(op.A.nx, op.A.ny, op.A.nz);
+  if (!op.A.fx && !op.A.fy && !op.A.fz) {
+    const int grid = quad_grid<DIM>(sg, (int64_t)dir_blocks_per_sm<DIM, true>() * 148);
+    launch(k_fcg_dir_q<DIM, true>, grid, Quad<DIM>::TX * Quad<DIM>::TY, 0, st, op.A, sg, s->S,
+           s->z32, s->p0, s->p1, s->q, s->r, s->partials, h);
+    return;
+  }
   const int grid = quad_grid<DIM>(sg, (int64_t)dir_blocks_per_sm<DIM>() * 148);
   launch(k_fcg_dir_q<DIM>, grid, Quad<DIM>::TX * Quad<DIM>::TY, 0, st, op.A, sg, s->S, s->z32,
          s->p0, s->p1, s->q, s->r, s->partials, h);
@@ -1609,9 +1616,15 @@ void launch_dir_q(LearnedSolver* s, const FineOperator& op, Loop h, cudaStream_t
 void launch_dir_s(LearnedSolver* s, const FineOperator& op, Loop h, cudaStream_t st) {
   const Seg sg = make_quad_seg<3>(op.A.nx, op.A.ny, op.A.nz);
   constexpr size_t SM = dir_s_smem();
-  const int grid = quad_wave<3>((const void*)k_dir_s, sg, SM);
-  launch(k_dir_s, grid, PlaneTile::T, SM, st, op.A, sg, s->S, s->z32, s->p0, s->p1, s->q, s->r,
-         s->partials, h);
+  // per-face arrays on all three axes, or the per-axis tables of a uniform operator
+  if (op.A.fx && op.A.fy && op.A.fz)
+    launch(k_dir_s<true>, quad_wave<3>((const void*)k_dir_s<true>, sg, SM), PlaneTile::T, SM, st,
+           op.A, sg, s->S, s->z32, s->p0, s->p1, s->q, s->r, s->partials, h);
+  else if (!op.A.fx && !op.A.fy && !op.A.fz)
+    launch(k_dir_s<false>, quad_wave<3>((const void*)k_dir_s<false>, sg, SM), PlaneTile::T, SM, st,
+           op.A, sg, s->S, s->z32, s->p0, s->p1, s->q, s->r, s->partials, h);
+  else
+    launch_dir_v<3>(s, op, h, st);
 }
 
 void launch_dir(LearnedSolver* s, const FineOperator& op, Loop h, cudaStream_t st) {

@@ -355,13 +355,15 @@ __global__ void __launch_bounds__(Quad<DIM>::TX* Quad<DIM>::TY)
 // The quad counterpart of the FCG direction pass (see k_fcg_dir).
 // Resident blocks per SM of the direction pass (its register budget); its
 // grid is one wave of them, so every block marches a long run of planes.
-template <int DIM>
+// TABLES: the operator's couplings are its per-axis tables (a uniform
+// operator), which needs fewer registers than the per-face form.
+template <int DIM, bool TABLES = false>
 constexpr int dir_blocks_per_sm() {
-  return DIM == 3 ? 2 : 8;
+  return DIM == 3 ? 2 : (TABLES ? 12 : 8);
 }
 
-template <int DIM>
-__global__ void __launch_bounds__(Quad<DIM>::TX* Quad<DIM>::TY, dir_blocks_per_sm<DIM>())
+template <int DIM, bool TABLES = false>
+__global__ void __launch_bounds__(Quad<DIM>::TX* Quad<DIM>::TY, dir_blocks_per_sm<DIM, TABLES>())
     k_fcg_dir_q(OpView<double> A, Seg sg, FcgState* S, const float* __restrict__ z, double* P0,
                 double* P1, double* __restrict__ q, const double* __restrict__ r, double* partials,
                 Loop h) {
@@ -404,7 +406,7 @@ __global__ void __launch_bounds__(Quad<DIM>::TX* Quad<DIM>::TY, dir_blocks_per_s
           const int64_t c = idx(i0, j, k);
           // couplings of the quad: per-face arrays or per-axis tables
           double fx[5];
-          if (A.fx) {
+          if (!TABLES && A.fx) {
             const int64_t bx = i0 + (int64_t)(A.nx + 1) * (j + (int64_t)A.ny * k);
 #pragma unroll
             for (int u = 0; u < 5; ++u) fx[u] = A.fx[bx + u];
@@ -413,7 +415,7 @@ __global__ void __launch_bounds__(Quad<DIM>::TX* Quad<DIM>::TY, dir_blocks_per_s
             for (int u = 0; u < 5; ++u) fx[u] = A.tx[i0 + u];
           }
           V4<double> yl, yh, zl, zh;
-          if (A.fy) {
+          if (!TABLES && A.fy) {
             const int64_t by = i0 + (int64_t)A.nx * (j + (int64_t)(A.ny + 1) * k);
             yl = ld4(A.fy + by);
             yh = ld4(A.fy + by + A.nx);
@@ -422,7 +424,7 @@ __global__ void __launch_bounds__(Quad<DIM>::TX* Quad<DIM>::TY, dir_blocks_per_s
             yl = V4<double>{{a, a, a, a}};
             yh = V4<double>{{bb, bb, bb, bb}};
           }
-          if (A.fz) {
+          if (!TABLES && A.fz) {
             zl = ld4(A.fz + c);
             zh = ld4(A.fz + c + (int64_t)A.nx * A.ny);
           } else {

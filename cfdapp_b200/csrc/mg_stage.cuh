@@ -438,8 +438,12 @@ constexpr size_t dir_s_smem() {
 // with the same arithmetic and coefficient order.  The z and p_old tiles
 // arrive by cp.async; the copying thread forms p in place once its copies
 // have landed; the couplings and r of the current plane are loaded before
-// the block waits for the plane.
-__global__ void __launch_bounds__(PlaneTile::T, 2)
+// the block waits for the plane.  FACES: per-face coupling arrays on all
+// axes (a p' system from a SIMPLE run); otherwise the per-axis tables of a
+// uniform operator, whose smaller register footprint lets three blocks
+// share an SM.
+template <bool FACES>
+__global__ void __launch_bounds__(PlaneTile::T, FACES ? 2 : 3)
     k_dir_s(OpView<double> A, Seg sg, FcgState* S, const float* __restrict__ z, double* P0,
             double* P1, double* __restrict__ q, const double* __restrict__ r, double* partials,
             Loop h) {
@@ -510,30 +514,23 @@ __global__ void __launch_bounds__(PlaneTile::T, 2)
       double fx[5];
       V4<double> yl, yh, zl, zh, rr = zero4<double>();
       if (act) {
-        if (A.fx) {
+        if (FACES) {
           const int64_t bx = i0 + (int64_t)(A.nx + 1) * (j + (int64_t)A.ny * k);
 #pragma unroll
           for (int u = 0; u < 5; ++u) fx[u] = A.fx[bx + u];
-        } else {
-#pragma unroll
-          for (int u = 0; u < 5; ++u) fx[u] = A.tx[i0 + u];
-        }
-        if (A.fy) {
           const int64_t by = i0 + (int64_t)A.nx * (j + (int64_t)(A.ny + 1) * k);
           yl = ld4(A.fy + by);
           yh = ld4(A.fy + by + A.nx);
-        } else {
-          const double a = A.ty[j], bb = A.ty[j + 1];
-          yl = V4<double>{{a, a, a, a}};
-          yh = V4<double>{{bb, bb, bb, bb}};
-        }
-        if (A.fz) {
           zl = ld4(A.fz + c);
           zh = ld4(A.fz + c + (int64_t)A.nx * A.ny);
         } else {
-          const double a = A.tz[k], bb = A.tz[k + 1];
-          zl = V4<double>{{a, a, a, a}};
-          zh = V4<double>{{bb, bb, bb, bb}};
+#pragma unroll
+          for (int u = 0; u < 5; ++u) fx[u] = A.tx[i0 + u];
+          const double ya = A.ty[j], yb = A.ty[j + 1], za = A.tz[k], zb = A.tz[k + 1];
+          yl = V4<double>{{ya, ya, ya, ya}};
+          yh = V4<double>{{yb, yb, yb, yb}};
+          zl = V4<double>{{za, za, za, za}};
+          zh = V4<double>{{zb, zb, zb, zb}};
         }
         rr = ld4(r + c);
       }
