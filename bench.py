@@ -175,8 +175,12 @@ GOLDEN = os.path.join(ROOT, "tests", "golden")
 # summaries are in profiles/ (learned_fcg_dram_traffic.md: the DRAM bytes of
 # one learned-FCG solve graph, mean of the 2048^2 and 256^3 solves;
 # batched_simple_64cases_iteration.md: the batched p' team kernel).
-NCU_TRAFFIC = {"learned_fcg_bytes_per_launch": 77140000000.0,
-               "batched_pprime_dram_bytes_per_launch": 521465025024.0}
+NCU_TRAFFIC = {"batched_pprime_dram_bytes_per_launch": 521465025024.0}
+# DRAM bytes of the learned-FCG solve graph of each benchmark system: its start
+# kernel plus one FCG iteration (learned_fcg_dram_traffic.md); a solve's
+# traffic is start + iterations x per_iteration.
+LEARNED_TRAFFIC = {(2, 2048): {"start": 0.08e9, "per_iteration": 0.6188e9},
+                   (3, 256): {"start": 0.47e9, "per_iteration": 3.168e9}}
 
 
 def reference_full_runs():
@@ -876,7 +880,11 @@ def main():
     kbytes = sum(r.krylov_bytes for rs in per_grid.values() for r in rs)
     klaunch = sum(r.krylov_launches for rs in per_grid.values() for r in rs)
     achieved = (kbytes / klaunch) / ((kms / klaunch) * 1e-3) / 1e9 if kms > 0 else None
-    traffic = NCU_TRAFFIC["learned_fcg_bytes_per_launch"]
+    # per solve-graph launch: the mean of the step's solves, each from the
+    # measured per-iteration traffic times its own iteration count
+    tr = [LEARNED_TRAFFIC[g]["start"] + r.iterations * LEARNED_TRAFFIC[g]["per_iteration"]
+          for g, rs in per_grid.items() if g in LEARNED_TRAFFIC for r in rs]
+    traffic = statistics.mean(tr) if tr else None
 
     grid_detail = {}
     for (dim, n), rs in per_grid.items():
