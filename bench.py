@@ -67,6 +67,8 @@ def parse():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32_refined"],
                     help="p' precision of --profile-solve and of the batched workload")
     ap.add_argument("--max-iterations", type=int, default=100000)
+    ap.add_argument("--batch-preconditioner", default="jacobi", choices=["jacobi", "learned_mg"],
+                    help="p' preconditioner of the batched workload")
     return ap.parse_args()
 
 
@@ -349,7 +351,7 @@ def batched_cases(seed, ncases):
     return out
 
 
-def batched_settings(precision="fp64"):
+def batched_settings(precision="fp64", preconditioner="jacobi"):
     from cfdapp_b200.cfdb import LinearSolverSettings, SIMPLESettings
     return SIMPLESettings(
         max_iterations=100000, velocity_relaxation=0.7, pressure_relaxation=0.3,
@@ -358,7 +360,7 @@ def batched_settings(precision="fp64"):
         momentum_solver=LinearSolverSettings(type="bicgstab", preconditioner="none",
                                              absolute_tolerance=1e-10, relative_tolerance=1e-8,
                                              max_iterations=500),
-        pressure_solver=LinearSolverSettings(type="cg", preconditioner="jacobi",
+        pressure_solver=LinearSolverSettings(type="cg", preconditioner=preconditioner,
                                              absolute_tolerance=0.0, relative_tolerance=1e-8,
                                              max_iterations=20000, precision=precision))
 
@@ -418,7 +420,8 @@ def run_batched_to_convergence(a, ctx, b, cases, cells, s):
         statuses[r["status"]] = statuses.get(r["status"], 0) + 1
     its = np.array([r["iterations"] for r in res])
     line = {"metric": "batched SIMPLE run to convergence", "cases": len(cases),
-            "pressure_precision": a.precision, "statuses": statuses,
+            "pressure_precision": a.precision, "pressure_preconditioner": a.batch_preconditioner,
+            "statuses": statuses,
             "outer_iterations": {"min": int(its.min()), "median": float(np.median(its)),
                                  "max": int(its.max())},
             "pressure_linear_iterations": int(sum(r["pressure_linear_iterations"] for r in res)),
@@ -447,7 +450,7 @@ def run_batched(a):
         raise SystemExit("bench.py: no sm_100 device visible (the product has no CPU path)")
     ctx = cfdb.Context(local)
     cases = batched_cases(SEED + rank, a.cases)
-    s = batched_settings(a.precision)
+    s = batched_settings(a.precision, a.batch_preconditioner)
     b = cfdb.Batch(ctx, [c[3] for c in cases], s)
     for k in range(len(cases)):
         b.set_state(k)
@@ -520,17 +523,25 @@ def run_batched(a):
             "config": {"workload": f"{len(cases)} uneven 2D SIMPLE cases per GPU (sides "
                                    f"{list(BATCH_SIDES)}, Re 100-1000, cavity or channel, "
                                    "seeded), upwind, linear flux, BiCGSTAB momentum, "
-                                   "Jacobi-PCG p' to 1e-8; one step = one outer iteration of "
-                                   "the whole batch (one CUDA graph launch)",
+                                   + ("learned-FCG p' to 1e-8 (case by case between two "
+                                      "CUDA graph launches)" if a.batch_preconditioner ==
+                                      "learned_mg" else
+                                      f"Jacobi-PCG p' ({a.precision}) to 1e-8") +
+                                   "; one step = one outer iteration of the whole batch",
                        "cells": int(cells.sum()), "l2": "inputs larger than L2",
                        "parallelism": f"independent batches x{world}"},
             "tuning": tuning.__dict__, "autotune_s": tune_s,
             "profiled_iteration_ms": stage_ms,
-            "roofline": {"bound": "hbm", "kernel": "batched p' Jacobi-CG team kernel",
-                         "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak if achieved else None,
-                         "peak_source": f"{peak_kind} hbm_gbs",
-                         "traffic": NCU_TRAFFIC["batched_pprime_dram_bytes_per_launch"]},
+            "roofline": ({"bound": "hbm", "kernel": "batched p' Jacobi-CG team kernel",
+                          "achieved": achieved, "peak": peak, "unit": "GB/s",
+                          "frac": achieved / peak if achieved else None,
+                          "peak_source": f"{peak_kind} hbm_gbs",
+                          "traffic": NCU_TRAFFIC["batched_pprime_dram_bytes_per_launch"]}
+                         if a.batch_preconditioner == "jacobi" else
+                         {"bound": "hbm", "kernel": "per-case learned-FCG p' solves (their "
+                          "roofline: the pprime workload)", "achieved": None, "peak": peak,
+                          "unit": "GB/s", "frac": None, "peak_source": f"{peak_kind} hbm_gbs",
+                          "traffic": None}),
             "e2e": {"value": e2e_work / (e2e_ms * 1e-3), "unit": "cell outer-iterations/s",
                     "h2d_bytes_per_step": h2d // max(a.steps, 1),
                     "d2h_bytes_per_step": d2h // max(a.steps, 1)},

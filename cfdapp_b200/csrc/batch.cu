@@ -25,6 +25,7 @@
 #include <vector>
 
 #include "batch.cuh"
+#include "pcg_internal.cuh"
 #include "cfdb.h"
 #include "cfdb_internal.cuh"
 #include "grid_sync.cuh"
@@ -183,6 +184,29 @@ __global__ void __launch_bounds__(krylov::kThreads, 5) k_batch_krylov(KArgs A) {
   }
 }
 
+// The learned p' solves' outcomes (lout: status, iterations, initial
+// residual per case, written by the host) applied with k_batch_krylov's
+// record rules: a case whose fields went non-finite stops with
+// NONFINITE_STATE, a p' solve that did not converge stops it with
+// PRESSURE_FAILURE.
+__global__ void k_batch_pp_record(BatchDev B, const double* __restrict__ lout) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < B.ncases; k += gridDim.x * blockDim.x) {
+    if (!B.active[k]) continue;
+    if (B.flags[(size_t)BF_NONFINITE * B.ncases + k] != 0u) {
+      B.status[k] = CFDB_SIMPLE_NONFINITE_STATE;
+      B.active[k] = 0;
+      continue;
+    }
+    if ((int)lout[3 * k] != CFDB_SOLVER_CONVERGED) {
+      B.status[k] = CFDB_SIMPLE_PRESSURE_FAILURE;
+      B.active[k] = 0;
+      continue;
+    }
+    B.res[(size_t)k * BR_COUNT + BR_IP] = lout[3 * k + 2];
+    B.p_it[k] += (int64_t)lout[3 * k + 1];
+  }
+}
+
 int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
 
 // Events around every launch of an eager profiling iteration; ids: stage
@@ -235,10 +259,25 @@ struct cfdb_batch {
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   int64_t history_cap = 0;
   Timeline* timeline = nullptr;  // set during a profiling iteration
+  // learned p' preconditioner: one p' operator per case, bound to the case's
+  // pooled face coefficients every outer iteration; the outer iteration is
+  // then two graphs around a host loop of the cases' learned solves
+  bool learned = false;
+  std::vector<cfdb_poperator*> pops;
+  cudaGraphExec_t exec_post = nullptr;
+  double* d_lout = nullptr;     // per case: status, iterations, initial residual
+  double* h_lout = nullptr;     // pinned mirror
+  unsigned* h_flags = nullptr;  // pinned mirror of the flags (BF_COUNT x n)
+  int* h_act = nullptr;         // pinned mirror of the active set
 
   ~cfdb_batch() {
     if (ctx) cudaStreamSynchronize(ctx->stream);
     if (exec) cudaGraphExecDestroy(exec);
+    if (exec_post) cudaGraphExecDestroy(exec_post);
+    for (cfdb_poperator* op : pops) cfdb_poperator_destroy(op);
+    if (h_lout) cudaFreeHost(h_lout);
+    if (h_flags) cudaFreeHost(h_flags);
+    if (h_act) cudaFreeHost(h_act);
     for (void* p : owned) cudaFree(p);
     if (h_nactive) cudaFreeHost(h_nactive);
     if (h_err) cudaFreeHost(h_err);
@@ -362,10 +401,8 @@ void enqueue_prefix(cfdb_batch* b, int record, cudaStream_t s) {
   launch_stage(b, BS_PROWS, 0, s);
 }
 
-void enqueue_iteration(cfdb_batch* b, cudaStream_t s) {
-  b->launches_per_iteration = 0;
-  enqueue_prefix(b, 1, s);
-  launch_krylov(b, 1, 0, 1, s);
+// The stages after the p' solve.
+void enqueue_suffix(cfdb_batch* b, cudaStream_t s) {
   launch_stage(b, BS_CHECK_PP, 0, s);
   launch_stage(b, BS_FACE_VALUES_PP, 0, s);
   launch_stage(b, BS_GG_PP, 0, s);
@@ -377,6 +414,59 @@ void enqueue_iteration(cfdb_batch* b, cudaStream_t s) {
   launch_stage(b, BS_CORRECT, 0, s);
   launch_stage(b, BS_FLUX_CORRECT, 0, s);
   launch_stage(b, BS_RESIDUAL, 0, s);
+}
+
+void enqueue_iteration(cfdb_batch* b, cudaStream_t s) {
+  b->launches_per_iteration = 0;
+  enqueue_prefix(b, 1, s);
+  launch_krylov(b, 1, 0, 1, s);
+  enqueue_suffix(b, s);
+}
+
+// With the learned p' preconditioner: the record of the host's p' outcomes,
+// then the stages after the p' solve.
+void enqueue_learned_post(cfdb_batch* b, cudaStream_t s) {
+  k_batch_pp_record<<<std::max(1, (b->n + 255) / 256), 256, 0, s>>>(b->D, b->d_lout);
+  b->launches_per_iteration += 1;
+  mark(b, -2, s);
+  enqueue_suffix(b, s);
+}
+
+// Every active case's p' system by the single-case learned solve, on its
+// pooled face coefficients, right-hand side and p' (zero) in place; the
+// outcomes go to d_lout.  The stages before (enqueue_prefix) must have run.
+cfdb_status run_learned_pprime(cfdb_batch* b) {
+  cfdb_context* ctx = b->ctx;
+  cudaStream_t s = ctx->stream;
+  const int n = b->n;
+  CFDB_CUDA(ctx, cudaMemcpyAsync(b->h_flags, b->D.flags, sizeof(unsigned) * BF_COUNT * (size_t)n,
+                                 cudaMemcpyDeviceToHost, s));
+  CFDB_CUDA(ctx, cudaMemcpyAsync(b->h_act, b->D.active, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost,
+                                 s));
+  CFDB_CUDA(ctx, cudaStreamSynchronize(s));
+  for (int k = 0; k < n; ++k) {
+    double* o = b->h_lout + 3 * (size_t)k;
+    o[0] = -1.0;
+    o[1] = 0.0;
+    o[2] = 0.0;
+    if (!b->h_act[k] || b->h_flags[(size_t)BF_NONFINITE * n + k] != 0u) continue;
+    if (b->h_flags[(size_t)BF_PP * n + k] & BFLAG_NONFINITE_INPUT) {
+      o[0] = CFDB_SOLVER_NONFINITE_INPUT;
+      continue;
+    }
+    cfdb_status rc = poperator_bind_faces(ctx, b->pops[k], b->D.D + b->hc[k].f0, false);
+    if (rc != CFDB_OK) return rc;
+    cfdb_linear_result r{};
+    rc = cfdb_poperator_solve_device(ctx, b->pops[k], &b->st.pressure, b->D.prhs + b->hc[k].c0,
+                                     b->D.pp + b->hc[k].c0, nullptr, 0, &r);
+    if (rc != CFDB_OK) return rc;
+    o[0] = r.status;
+    o[1] = (double)r.iterations;
+    o[2] = r.initial_residual;
+  }
+  CFDB_CUDA(ctx, cudaMemcpyAsync(b->d_lout, b->h_lout, sizeof(double) * 3 * (size_t)n,
+                                 cudaMemcpyHostToDevice, s));
+  return CFDB_OK;
 }
 
 cfdb_status upload_tiles(cfdb_batch* b) {
@@ -456,14 +546,29 @@ cfdb_status build_graph(cfdb_batch* b) {
     occupancy(b, st, b->tune.cell_threads);
     occupancy(b, st, b->tune.face_threads);
   }
-  cudaGraph_t g = nullptr;
-  CFDB_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-  enqueue_iteration(b, ctx->stream);
-  cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
-  if (e != cudaSuccess) return cuda_error(ctx, e, "batch graph capture", __FILE__, __LINE__);
-  e = cudaGraphInstantiate(&b->exec, g, 0);
-  cudaGraphDestroy(g);
-  if (e != cudaSuccess) return cuda_error(ctx, e, "batch graph instantiation", __FILE__, __LINE__);
+  if (b->exec_post) {
+    cudaGraphExecDestroy(b->exec_post);
+    b->exec_post = nullptr;
+  }
+  auto capture = [&](cudaGraphExec_t* out, auto body) -> cfdb_status {
+    cudaGraph_t g = nullptr;
+    CFDB_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    body();
+    cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+    if (e != cudaSuccess) return cuda_error(ctx, e, "batch graph capture", __FILE__, __LINE__);
+    e = cudaGraphInstantiate(out, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_error(ctx, e, "batch graph instantiation", __FILE__, __LINE__);
+    return CFDB_OK;
+  };
+  cfdb_status rc;
+  if (b->learned) {
+    b->launches_per_iteration = 0;
+    if ((rc = capture(&b->exec, [&] { enqueue_prefix(b, 1, ctx->stream); }))) return rc;
+    if ((rc = capture(&b->exec_post, [&] { enqueue_learned_post(b, ctx->stream); }))) return rc;
+  } else if ((rc = capture(&b->exec, [&] { enqueue_iteration(b, ctx->stream); }))) {
+    return rc;
+  }
   b->dirty = false;
   return CFDB_OK;
 }
@@ -581,10 +686,14 @@ cfdb_status cfdb_batch_create(cfdb_context* ctx, int ncases, const cfdb_simple_c
       st->momentum.max_iterations < 1 || st->pressure.max_iterations < 1)
     return set_error(ctx, CFDB_ERR_INVALID_ARGUMENT, "invalid relaxation or iteration limits");
   for (const cfdb_linear_settings* L : {&st->momentum, &st->pressure}) {
-    if ((L->preconditioner != CFDB_PRECOND_NONE && L->preconditioner != CFDB_PRECOND_JACOBI) ||
+    const bool learned_pp = L == &st->pressure && L->preconditioner == CFDB_PRECOND_LEARNED_MG &&
+                            L->krylov == CFDB_KRYLOV_CG && L->precision == CFDB_PRECISION_FP64;
+    if ((L->preconditioner != CFDB_PRECOND_NONE && L->preconditioner != CFDB_PRECOND_JACOBI &&
+         !learned_pp) ||
         (L->krylov != CFDB_KRYLOV_CG && L->krylov != CFDB_KRYLOV_BICGSTAB))
       return set_error(ctx, CFDB_ERR_UNSUPPORTED,
-                       "batched solves support CG/BiCGSTAB with no or Jacobi preconditioning");
+                       "batched solves support CG/BiCGSTAB with no or Jacobi preconditioning, "
+                       "or an FP64 CG p' solve with the learned preconditioner");
     const bool mixed_pp = L == &st->pressure && L->krylov == CFDB_KRYLOV_CG &&
                           L->precision == CFDB_PRECISION_FP32_REFINED;
     if (L->precision != CFDB_PRECISION_FP64 && !mixed_pp)
@@ -719,6 +828,18 @@ cfdb_status cfdb_batch_create(cfdb_context* ctx, int ncases, const cfdb_simple_c
   *b->h_nactive = ncases;
   CFDB_CUDA(ctx, cudaEventCreate(&b->e0));
   CFDB_CUDA(ctx, cudaEventCreate(&b->e1));
+  if (st->pressure.preconditioner == CFDB_PRECOND_LEARNED_MG) {
+    b->learned = true;
+    if ((rc = dalloc(b.get(), &b->d_lout, 3 * (size_t)ncases))) return rc;
+    CFDB_CUDA(ctx, cudaMallocHost((void**)&b->h_lout, sizeof(double) * 3 * ncases));
+    CFDB_CUDA(ctx, cudaMallocHost((void**)&b->h_flags, sizeof(unsigned) * BF_COUNT * ncases));
+    CFDB_CUDA(ctx, cudaMallocHost((void**)&b->h_act, sizeof(int) * ncases));
+    b->pops.assign(ncases, nullptr);
+    for (int k = 0; k < ncases; ++k)
+      if ((rc = cfdb_poperator_create_uniform(ctx, &cases[k].grid, 1.0, 0u, b->hc[k].pin,
+                                              b->hc[k].ref, &b->pops[k])))
+        return rc;
+  }
   cfdb_batch_tuning t{};
   t.cell_threads = 256;
   t.cell_tile = 1024;
@@ -823,6 +944,12 @@ cfdb_status cfdb_batch_iterate(cfdb_batch* b, int64_t nmax, cfdb_batch_stats* st
   for (int64_t it = 0; it < nmax && nact > 0; ++it) {
     CFDB_CUDA(ctx, cudaEventRecord(b->e0, s));
     CFDB_CUDA(ctx, cudaGraphLaunch(b->exec, s));
+    if (b->learned) {
+      const int64_t l0 = ctx->launches;
+      if ((rc = run_learned_pprime(b))) return rc;
+      S.kernel_launches += ctx->launches - l0;
+      CFDB_CUDA(ctx, cudaGraphLaunch(b->exec_post, s));
+    }
     CFDB_CUDA(ctx, cudaEventRecord(b->e1, s));
     CFDB_CUDA(ctx, cudaMemcpyAsync(b->h_nactive, b->D.nactive, sizeof(int), cudaMemcpyDeviceToHost, s));
     CFDB_CUDA(ctx, cudaMemcpyAsync(b->h_err, b->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
@@ -873,7 +1000,17 @@ cfdb_status cfdb_batch_profile_iteration(cfdb_batch* b, int* ids, double* ms, in
   Timeline tl;
   b->timeline = &tl;
   mark(b, -100, s);
-  enqueue_iteration(b, s);
+  if (b->learned) {
+    b->launches_per_iteration = 0;
+    enqueue_prefix(b, 1, s);
+    if ((rc = run_learned_pprime(b))) {
+      b->timeline = nullptr;
+      return rc;
+    }
+    enqueue_learned_post(b, s);
+  } else {
+    enqueue_iteration(b, s);
+  }
   b->timeline = nullptr;
   b->dirty = true;  // the graph's launch count is re-counted at its next capture
   cudaError_t e = cudaStreamSynchronize(s);

@@ -403,8 +403,10 @@ CFDB_API cfdb_status cfdb_simple_write_results(cfdb_simple* s, const double* his
  * keeps one Krylov space: FP32 matrix copy, direction and A p; FP64 x, r and
  * reductions; the FP64 true residual replaces the recurrence after every
  * ten-fold drop, at the tolerance and at the cap; inner_rel_tol and
- * max_refinements are not used), uniform grids (others return
- * CFDB_ERR_UNSUPPORTED). */
+ * max_refinements are not used), or, for an FP64 CG p' solve,
+ * CFDB_PRECOND_LEARNED_MG (every active case's p' system by the single-case
+ * learned FCG, case by case, between two graph launches of the stages),
+ * uniform grids (others return CFDB_ERR_UNSUPPORTED). */
 typedef struct cfdb_batch cfdb_batch;
 
 /* Launch shapes of the batch: cells (faces) per tile and threads per block

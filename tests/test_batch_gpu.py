@@ -209,10 +209,10 @@ def test_batch_edge_cases(ctx):
     one.close()
     with pytest.raises(CfdbError):
         Batch(ctx, [SimpleCase.cavity(2, 8), SimpleCase.cavity(3, 6)], s)
-    learned = SIMPLESettings(max_iterations=8, pressure_solver=LinearSolverSettings(
-        type="cg", preconditioner="learned_mg"))
+    learned_bicgstab = SIMPLESettings(max_iterations=8, pressure_solver=LinearSolverSettings(
+        type="bicgstab", preconditioner="learned_mg"))
     with pytest.raises(CfdbError):
-        Batch(ctx, [SimpleCase.cavity(2, 8)], learned)
+        Batch(ctx, [SimpleCase.cavity(2, 8)], learned_bicgstab)
 
 
 @pytest.mark.parametrize("name", ["cavity2d_16_jacobicg", "cavity3d_32_lud_rc_re1000"])
@@ -236,6 +236,37 @@ def test_batch_mixed_precision_pprime_matches_reference(ctx, name):
     r = b.results()[1]
     assert r["status"] == meta["status"] == "Converged"
     assert abs(r["iterations"] - meta["iterations"]) <= max(2, 0.02 * meta["iterations"])
+    u, v, w, p, f = b.get_state(1)
+    for fld, arr in (("u", u), ("v", v), ("w", w), ("p", p)):
+        if fld in g.files:
+            assert _rel(arr, g[fld]) <= 1e-6, fld
+    assert _rel(f, g["flux"]) <= 1e-6
+    assert b.results()[0]["status"] == "Converged"
+    b.close()
+
+
+@pytest.mark.parametrize("name", ["cavity2d_16_jacobicg", "cavity3d_32_lud_rc_re1000"])
+def test_batch_learned_pprime_matches_reference(ctx, name):
+    """The batch's learned p' solve (every active case's p' system by the
+    single-case learned FCG on the case's pooled face coefficients): the
+    golden case lands on the reference's fields with the bar of the
+    single-case learned SIMPLE test (outer iterations within 3 %, fields within
+    1e-6 relative L2), and the other case converges."""
+    from cfdapp_b200.cfdb import Batch
+    import dataclasses
+    g, meta = _golden(name)
+    case, s = gpu_case_from_args(meta["args"])
+    s = dataclasses.replace(s, pressure_solver=dataclasses.replace(s.pressure_solver,
+                                                                  preconditioner="learned_mg"))
+    other = gpu_case_from_args(_extras(meta["args"])[0])[0]
+    b = Batch(ctx, [other, case], s)
+    for k in range(2):
+        b.set_state(k)
+    st = b.iterate(s.max_iterations)
+    assert st["kernel_launches"] > 0
+    r = b.results()[1]
+    assert r["status"] == meta["status"] == "Converged"
+    assert abs(r["iterations"] - meta["iterations"]) <= max(3, 0.03 * meta["iterations"])
     u, v, w, p, f = b.get_state(1)
     for fld, arr in (("u", u), ("v", v), ("w", w), ("p", p)):
         if fld in g.files:
