@@ -1492,12 +1492,15 @@ cfdb_status mg_build(cfdb_context* ctx, MgHierarchy& H, const FineOperator& op) 
     --cf;
   H.coarse_from = cf;
   H.coarse_smem = coarse_bytes(H, cf);
+  // opted in to the largest tail any hierarchy may have, so that hierarchies
+  // of other sizes (other operators, other host threads) never lower it
+  // under a launch of this one
   if (op.dim == 2)
     CFDB_CUDA(ctx, cudaFuncSetAttribute(k_coarse<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)H.coarse_smem));
+                                        (int)kCoarseSmemCap));
   else
     CFDB_CUDA(ctx, cudaFuncSetAttribute(k_coarse<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)H.coarse_smem));
+                                        (int)kCoarseSmemCap));
   return refresh_values(ctx, H, op);
 }
 
