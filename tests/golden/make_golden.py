@@ -41,6 +41,9 @@ SIMPLE = {
     # Jacobi-CG p' to 1e-8) on a 32^3 cavity, to convergence
     "cavity3d_32_lud_rc_re1000": ("dim=3 nx=32 ny=32 nz=32 mu=0.001 scheme=lud flux=rhiechow "
                                   "outer=5000", ["u", "v", "w", "p", "flux"]),
+    # the same at 48^3
+    "cavity3d_48_lud_rc_re1000": ("dim=3 nx=48 ny=48 nz=48 mu=0.001 scheme=lud flux=rhiechow "
+                                  "outer=5000", ["u", "v", "w", "p", "flux"]),
     # rectilinear (graded) meshes, createGraded2D with geometric ratios: the
     # node coordinates are stored with the fields
     "cavity2d_24_graded": ("dim=2 nx=24 ny=24 gradex=1.12 gradey=1.12 outer=20000",

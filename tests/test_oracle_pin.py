@@ -69,12 +69,12 @@ def test_poisson_matches_golden(name):
 # (the 129^2 configuration-1 run takes the CPU restatement about an hour: it
 # pins the GPU path only, tests/test_simple_gpu.py)
 # (the oracle restates uniform grids: the graded-mesh fixtures pin the GPU
-# path directly; the 32^3 LUD + Rhie-Chow run takes the CPU restatement
-# minutes, like the 129^2 one: both pin the GPU path only)
+# path directly; the 32^3 and 48^3 LUD + Rhie-Chow runs take the CPU
+# restatement minutes, like the 129^2 one: they pin the GPU path only)
 @pytest.mark.parametrize("name", [n for n in _fixtures("")
                                   if not n.startswith(("poisson", "results_", "csr_", "fullsize_"))
                                   and "_129_" not in n and "graded" not in n
-                                  and not n.startswith("cavity3d_32")])
+                                  and not n.startswith(("cavity3d_32", "cavity3d_48"))])
 def test_simple_matches_golden(name):
     g = np.load(os.path.join(GOLDEN, name + ".npz"))
     meta = json.loads(str(g["meta"]))

@@ -118,9 +118,9 @@ def _golden(name):
 @pytest.mark.parametrize("name", ["cavity2d_20_bicgstab", "cavity2d_16_jacobicg",
                                   "channel2d_32x8_central_rc", "cavity2d_16_lud",
                                   "cavity3d_8_quick_rc", "cavity2d_129_config1",
-                                  "cavity3d_32_lud_rc_re1000", "cavity2d_33_jacobicg",
-                                  "cavity2d_24_graded", "cavity2d_24_graded_lud_rc",
-                                  "channel2d_32x12_graded"])
+                                  "cavity3d_32_lud_rc_re1000", "cavity3d_48_lud_rc_re1000",
+                                  "cavity2d_33_jacobicg", "cavity2d_24_graded",
+                                  "cavity2d_24_graded_lud_rc", "channel2d_32x12_graded"])
 def test_simple_matches_reference_outputs(ctx, name):
     from cfdapp_b200.cfdb import simple_solve
     g, meta = _golden(name)
@@ -160,7 +160,7 @@ def test_simple_failure_statuses(ctx):
 @pytest.mark.parametrize("name", ["cavity2d_16_jacobicg", "channel2d_32x8_central_rc",
                                   "cavity2d_16_lud", "cavity3d_8_quick_rc",
                                   "cavity2d_129_config1", "cavity3d_32_lud_rc_re1000",
-                                  "cavity2d_24_graded"])
+                                  "cavity3d_48_lud_rc_re1000", "cavity2d_24_graded"])
 def test_simple_with_learned_pressure_solver_matches_reference(ctx, name):
     """The same SIMPLE runs with every p' system solved by the learned-
     preconditioned FCG (to the same tolerance) land on the reference's fields."""
