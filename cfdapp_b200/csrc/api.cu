@@ -92,8 +92,11 @@ cfdb_status cfdb_create(int device, void* stream, cfdb_context** out) {
   }
   if ((e = cudaMalloc((void**)&ctx->sync_words, 16 * sizeof(unsigned))) != cudaSuccess)
     return fail(e, "cudaMalloc");
-  if ((e = cudaMemset(ctx->sync_words, 0, 16 * sizeof(unsigned))) != cudaSuccess)
-    return fail(e, "cudaMemset");
+  // on the context's (non-blocking) stream, then waited for, so that no later
+  // work of the context can run ahead of the clear
+  if ((e = cudaMemsetAsync(ctx->sync_words, 0, 16 * sizeof(unsigned), ctx->stream)) != cudaSuccess ||
+      (e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess)
+    return fail(e, "cudaMemsetAsync");
   if ((e = cudaMalloc((void**)&ctx->scalars, 64 * sizeof(double))) != cudaSuccess)
     return fail(e, "cudaMalloc");
   if ((e = cudaMallocHost((void**)&ctx->scalars_host, 64 * sizeof(double))) != cudaSuccess)

@@ -1756,9 +1756,14 @@ cfdb_status ensure_state(cfdb_context* ctx, LearnedSolver* s, const FineOperator
       s->free_all();
       return st;
     }
+    // cleared on the context's own stream: the context streams are
+    // non-blocking, so a legacy-stream memset would not be ordered before the
+    // solve's own writes of the state (and could land after them)
     cudaError_t e1 = cudaMalloc((void**)&s->S, sizeof(FcgState));
-    cudaError_t e2 = e1 == cudaSuccess ? cudaMemset(s->S, 0, sizeof(FcgState)) : e1;
-    cudaError_t e3 = e2 == cudaSuccess ? cudaMemset(s->q, 0, sizeof(double) * cells) : e2;
+    cudaError_t e2 =
+        e1 == cudaSuccess ? cudaMemsetAsync(s->S, 0, sizeof(FcgState), ctx->stream) : e1;
+    cudaError_t e3 =
+        e2 == cudaSuccess ? cudaMemsetAsync(s->q, 0, sizeof(double) * cells, ctx->stream) : e2;
     cudaError_t e4 = e3 == cudaSuccess ? cudaMallocHost((void**)&s->S_host, sizeof(FcgState)) : e3;
     cudaError_t e5 = e4 == cudaSuccess ? cudaStreamCreateWithFlags(&s->cap, cudaStreamNonBlocking) : e4;
     if (e5 != cudaSuccess) {

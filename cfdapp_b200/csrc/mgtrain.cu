@@ -348,7 +348,10 @@ struct Trainer {
     std::vector<TL> h(H.levels);
     for (int l = 0; l < H.levels; ++l) h[l] = tl(H.L[l]);
     if (cudaMalloc((void**)&d_tl, sizeof(TL) * H.levels) != cudaSuccess) return false;
-    if (cudaMemcpy(d_tl, h.data(), sizeof(TL) * H.levels, cudaMemcpyHostToDevice) != cudaSuccess)
+    // stream-ordered: the context stream is non-blocking
+    if (cudaMemcpyAsync(d_tl, h.data(), sizeof(TL) * H.levels, cudaMemcpyHostToDevice, st) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
       return false;
     if (cudaMalloc((void**)&d_acc, sizeof(double) * (16 * 27 + 16 + 2)) != cudaSuccess) return false;
     return err == cudaSuccess;

@@ -972,8 +972,13 @@ cfdb_status build_tables(cfdb_context* ctx, cfdb_poperator* op, double rho, unsi
     for (size_t i = 0; i < m; ++i) t32[i] = (float)tab[q][i];
     CFDB_CUDA(ctx, cudaMalloc((void**)&op->t64[q], m * sizeof(double)));
     CFDB_CUDA(ctx, cudaMalloc((void**)&op->t32[q], m * sizeof(float)));
-    CFDB_CUDA(ctx, cudaMemcpy(op->t64[q], tab[q].data(), m * sizeof(double), cudaMemcpyHostToDevice));
-    CFDB_CUDA(ctx, cudaMemcpy(op->t32[q], t32.data(), m * sizeof(float), cudaMemcpyHostToDevice));
+    // stream-ordered (the context stream is non-blocking): the solves that
+    // read the tables run on the same stream
+    CFDB_CUDA(ctx, cudaMemcpyAsync(op->t64[q], tab[q].data(), m * sizeof(double),
+                                   cudaMemcpyHostToDevice, ctx->stream));
+    CFDB_CUDA(ctx, cudaMemcpyAsync(op->t32[q], t32.data(), m * sizeof(float), cudaMemcpyHostToDevice,
+                                   ctx->stream));
+    CFDB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   }
   return CFDB_OK;
 }
@@ -1105,9 +1110,12 @@ cfdb_status upload_faces(cfdb_context* ctx, cfdb_poperator* op, const double* fa
       if (e1 != cudaSuccess || e2 != cudaSuccess)
         return set_error(ctx, CFDB_ERR_OUT_OF_MEMORY, "face coefficient allocation failed");
     }
-    CFDB_CUDA(ctx, cudaMemcpy(op->f64[ka], face_coeff_host + offs[a], m * sizeof(double),
-                              cudaMemcpyHostToDevice));
-    CFDB_CUDA(ctx, cudaMemcpy(op->f32[ka], f32.data(), m * sizeof(float), cudaMemcpyHostToDevice));
+    // stream-ordered behind the context's earlier solves and ahead of its next
+    CFDB_CUDA(ctx, cudaMemcpyAsync(op->f64[ka], face_coeff_host + offs[a], m * sizeof(double),
+                                   cudaMemcpyHostToDevice, ctx->stream));
+    CFDB_CUDA(ctx, cudaMemcpyAsync(op->f32[ka], f32.data(), m * sizeof(float), cudaMemcpyHostToDevice,
+                                   ctx->stream));
+    CFDB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   }
   if (alloc) {
     CFDB_CUDA(ctx, cudaMalloc((void**)&op->invd64, sizeof(double) * (size_t)op->cells));

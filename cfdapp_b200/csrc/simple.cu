@@ -470,7 +470,7 @@ cfdb_status cfdb_simple_create(cfdb_context* ctx, const cfdb_simple_case* cs,
     if (s->cs.nodes[a]) {
       const size_t bytes = sizeof(double) * s->hnodes[a].size();
       CFDB_CUDA(ctx, cudaMalloc((void**)&s->dnodes[a], bytes));
-      CFDB_CUDA(ctx, cudaMemcpy(s->dnodes[a], s->hnodes[a].data(), bytes, cudaMemcpyHostToDevice));
+      CFDB_CUDA(ctx, cudaMemcpyAsync(s->dnodes[a], s->hnodes[a].data(), bytes, cudaMemcpyHostToDevice, ctx->stream));
       s->G.node[a] = s->dnodes[a];  // the kernels read the device copy
     }
   s->n = s->G.nc;
@@ -510,10 +510,10 @@ cfdb_status cfdb_simple_create(cfdb_context* ctx, const cfdb_simple_case* cs,
   CFDB_CUDA(ctx, cudaMalloc((void**)&s->d_pctype, 6 * sizeof(int)));
   CFDB_CUDA(ctx, cudaMalloc((void**)&s->d_pcvalue, 6 * sizeof(double)));
   CFDB_CUDA(ctx, cudaMalloc((void**)&s->flag, sizeof(unsigned)));
-  CFDB_CUDA(ctx, cudaMemcpy(s->d_ptype, cs->pbc_type, 6 * sizeof(int), cudaMemcpyHostToDevice));
-  CFDB_CUDA(ctx, cudaMemcpy(s->d_pvalue, cs->pbc_value, 6 * sizeof(double), cudaMemcpyHostToDevice));
-  CFDB_CUDA(ctx, cudaMemcpy(s->d_pctype, pct, 6 * sizeof(int), cudaMemcpyHostToDevice));
-  CFDB_CUDA(ctx, cudaMemcpy(s->d_pcvalue, pcv, 6 * sizeof(double), cudaMemcpyHostToDevice));
+  CFDB_CUDA(ctx, cudaMemcpyAsync(s->d_ptype, cs->pbc_type, 6 * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+  CFDB_CUDA(ctx, cudaMemcpyAsync(s->d_pvalue, cs->pbc_value, 6 * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  CFDB_CUDA(ctx, cudaMemcpyAsync(s->d_pctype, pct, 6 * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+  CFDB_CUDA(ctx, cudaMemcpyAsync(s->d_pcvalue, pcv, 6 * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
   CFDB_CUDA(ctx, cudaEventCreate(&s->e0));
   CFDB_CUDA(ctx, cudaEventCreate(&s->e1));
   rc = cfdb_poperator_create_uniform(ctx, &cs->grid, 1.0, 0u, s->pin, st->reference_cell, &s->pop);
