@@ -21,6 +21,8 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <string>
+#include <thread>
 #include <utility>
 #include <vector>
 
@@ -37,6 +39,9 @@ namespace {
 
 constexpr unsigned long long kTeamTimeoutNs = 2000000000ull;
 constexpr int kKoutStride = 8;
+// Host threads (each with its own context and stream) that run the learned
+// p' solves of a batch's cases concurrently.
+constexpr int kLearnedWorkers = 8;
 constexpr int64_t kMinCellsPerBlock = 2048;
 constexpr int kAlign = 32;  // elements: every case starts on a 256-byte boundary
 
@@ -263,6 +268,7 @@ struct cfdb_batch {
   // pooled face coefficients every outer iteration; the outer iteration is
   // then two graphs around a host loop of the cases' learned solves
   bool learned = false;
+  std::vector<cfdb_context*> wctx;  // worker contexts (own streams); case k on wctx[k % size]
   std::vector<cfdb_poperator*> pops;
   cudaGraphExec_t exec_post = nullptr;
   double* d_lout = nullptr;     // per case: status, iterations, initial residual
@@ -275,6 +281,7 @@ struct cfdb_batch {
     if (exec) cudaGraphExecDestroy(exec);
     if (exec_post) cudaGraphExecDestroy(exec_post);
     for (cfdb_poperator* op : pops) cfdb_poperator_destroy(op);
+    for (cfdb_context* w : wctx) cfdb_destroy(w);
     if (h_lout) cudaFreeHost(h_lout);
     if (h_flags) cudaFreeHost(h_flags);
     if (h_act) cudaFreeHost(h_act);
@@ -435,6 +442,10 @@ void enqueue_learned_post(cfdb_batch* b, cudaStream_t s) {
 // Every active case's p' system by the single-case learned solve, on its
 // pooled face coefficients, right-hand side and p' (zero) in place; the
 // outcomes go to d_lout.  The stages before (enqueue_prefix) must have run.
+// The cases are shared among the worker contexts, each on its own host
+// thread and stream, so several solves run on the GPU at once; every solve
+// synchronises its own stream, and the host has synchronised the batch's
+// stream before, so the work is ordered against both graphs.
 cfdb_status run_learned_pprime(cfdb_batch* b) {
   cfdb_context* ctx = b->ctx;
   cudaStream_t s = ctx->stream;
@@ -444,25 +455,51 @@ cfdb_status run_learned_pprime(cfdb_batch* b) {
   CFDB_CUDA(ctx, cudaMemcpyAsync(b->h_act, b->D.active, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost,
                                  s));
   CFDB_CUDA(ctx, cudaStreamSynchronize(s));
-  for (int k = 0; k < n; ++k) {
-    double* o = b->h_lout + 3 * (size_t)k;
-    o[0] = -1.0;
-    o[1] = 0.0;
-    o[2] = 0.0;
-    if (!b->h_act[k] || b->h_flags[(size_t)BF_NONFINITE * n + k] != 0u) continue;
-    if (b->h_flags[(size_t)BF_PP * n + k] & BFLAG_NONFINITE_INPUT) {
-      o[0] = CFDB_SOLVER_NONFINITE_INPUT;
-      continue;
+  const int nw = (int)b->wctx.size();
+  std::vector<cfdb_status> wrc(nw, CFDB_OK);
+  std::vector<int64_t> l0(nw);
+  for (int w = 0; w < nw; ++w) l0[w] = b->wctx[w]->launches;
+  auto work = [&](int w) {
+    cfdb_context* wc = b->wctx[w];
+    if (cudaSetDevice(wc->device) != cudaSuccess) {
+      wrc[w] = set_error(wc, CFDB_ERR_CUDA, "cudaSetDevice on a batch worker thread");
+      return;
     }
-    cfdb_status rc = poperator_bind_faces(ctx, b->pops[k], b->D.D + b->hc[k].f0, false);
-    if (rc != CFDB_OK) return rc;
-    cfdb_linear_result r{};
-    rc = cfdb_poperator_solve_device(ctx, b->pops[k], &b->st.pressure, b->D.prhs + b->hc[k].c0,
-                                     b->D.pp + b->hc[k].c0, nullptr, 0, &r);
-    if (rc != CFDB_OK) return rc;
-    o[0] = r.status;
-    o[1] = (double)r.iterations;
-    o[2] = r.initial_residual;
+    for (int k = w; k < n; k += nw) {
+      double* o = b->h_lout + 3 * (size_t)k;
+      o[0] = -1.0;
+      o[1] = 0.0;
+      o[2] = 0.0;
+      if (!b->h_act[k] || b->h_flags[(size_t)BF_NONFINITE * n + k] != 0u) continue;
+      if (b->h_flags[(size_t)BF_PP * n + k] & BFLAG_NONFINITE_INPUT) {
+        o[0] = CFDB_SOLVER_NONFINITE_INPUT;
+        continue;
+      }
+      cfdb_status rc = poperator_bind_faces(wc, b->pops[k], b->D.D + b->hc[k].f0, false);
+      cfdb_linear_result r{};
+      if (rc == CFDB_OK)
+        rc = cfdb_poperator_solve_device(wc, b->pops[k], &b->st.pressure, b->D.prhs + b->hc[k].c0,
+                                         b->D.pp + b->hc[k].c0, nullptr, 0, &r);
+      if (rc != CFDB_OK) {
+        wrc[w] = rc;
+        return;
+      }
+      o[0] = r.status;
+      o[1] = (double)r.iterations;
+      o[2] = r.initial_residual;
+    }
+  };
+  {
+    std::vector<std::thread> threads;
+    for (int w = 1; w < nw; ++w) threads.emplace_back(work, w);
+    work(0);
+    for (std::thread& t : threads) t.join();
+  }
+  for (int w = 0; w < nw; ++w) {
+    ctx->launches += b->wctx[w]->launches - l0[w];
+    if (wrc[w] != CFDB_OK)
+      return set_error(ctx, wrc[w], std::string("learned p' solve of a batched case: ") +
+                                        b->wctx[w]->last_error);
   }
   CFDB_CUDA(ctx, cudaMemcpyAsync(b->d_lout, b->h_lout, sizeof(double) * 3 * (size_t)n,
                                  cudaMemcpyHostToDevice, s));
@@ -834,11 +871,19 @@ cfdb_status cfdb_batch_create(cfdb_context* ctx, int ncases, const cfdb_simple_c
     CFDB_CUDA(ctx, cudaMallocHost((void**)&b->h_lout, sizeof(double) * 3 * ncases));
     CFDB_CUDA(ctx, cudaMallocHost((void**)&b->h_flags, sizeof(unsigned) * BF_COUNT * ncases));
     CFDB_CUDA(ctx, cudaMallocHost((void**)&b->h_act, sizeof(int) * ncases));
+    // worker contexts for concurrent per-case solves (their own streams)
+    const int nw = std::min(kLearnedWorkers, ncases);
+    for (int w = 0; w < nw; ++w) {
+      cfdb_context* wc = nullptr;
+      if ((rc = cfdb_create(ctx->device, nullptr, &wc)) != CFDB_OK)
+        return set_error(ctx, rc, "batch worker context");
+      b->wctx.push_back(wc);
+    }
     b->pops.assign(ncases, nullptr);
     for (int k = 0; k < ncases; ++k)
-      if ((rc = cfdb_poperator_create_uniform(ctx, &cases[k].grid, 1.0, 0u, b->hc[k].pin,
-                                              b->hc[k].ref, &b->pops[k])))
-        return rc;
+      if ((rc = cfdb_poperator_create_uniform(b->wctx[k % nw], &cases[k].grid, 1.0, 0u,
+                                              b->hc[k].pin, b->hc[k].ref, &b->pops[k])))
+        return set_error(ctx, rc, b->wctx[k % nw]->last_error);
   }
   cfdb_batch_tuning t{};
   t.cell_threads = 256;
