@@ -490,9 +490,17 @@ cfdb_status run_learned_pprime(cfdb_batch* b) {
     }
   };
   {
+    // a worker whose thread cannot be started runs on this thread afterwards
     std::vector<std::thread> threads;
-    for (int w = 1; w < nw; ++w) threads.emplace_back(work, w);
-    work(0);
+    std::vector<int> here = {0};
+    for (int w = 1; w < nw; ++w) {
+      try {
+        threads.emplace_back(work, w);
+      } catch (...) {
+        here.push_back(w);
+      }
+    }
+    for (int w : here) work(w);
     for (std::thread& t : threads) t.join();
   }
   for (int w = 0; w < nw; ++w) {
