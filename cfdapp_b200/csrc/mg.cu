@@ -102,6 +102,30 @@ __device__ __forceinline__ void pdl_enter() {
   asm volatile("griddepcontrol.wait;" ::: "memory");
 }
 
+// 16-, 8- and 4-byte asynchronous global -> shared copies (cp.async); a copy
+// whose source lies outside the level fills its bytes with zeros and reads
+// nothing.
+__device__ __forceinline__ void cp16(void* dst, const void* src, bool in) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(src), "r"(in ? 16 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp8(void* dst, const void* src, bool in) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(src), "r"(in ? 8 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp4(void* dst, const void* src, bool in) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(src), "r"(in ? 4 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
 // Thread layout of the tiled kernels: TX x TY threads, each owning CX cells
 // of a plane row strided by TX (so every load instruction is coalesced).
 template <int DIM>
@@ -602,144 +626,199 @@ struct CoarsePlan {
   float cw[kMaxCoarse];
 };
 
-template <int DIM>
-__device__ __forceinline__ float lap_s(const LV& M, int i, int j, int k, int c, const float* x) {
-  const C7 co = coef<DIM>(M, i, j, k);
-  const int plane = M.nx * M.ny;
-  const float w = i > 0 ? x[c - 1] : 0.f, e = i + 1 < M.nx ? x[c + 1] : 0.f;
-  const float s = (DIM == 3 && j > 0) ? x[c - M.nx] : 0.f;
-  const float n = (DIM == 3 && j + 1 < M.ny) ? x[c + M.nx] : 0.f;
-  const float b = k > 0 ? x[c - plane] : 0.f, t = k + 1 < M.nz ? x[c + plane] : 0.f;
-  return apply7(co, x[c], w, e, s, n, b, t);
+// Cells of a padded shared-memory vector (x, res): one zero cell past each
+// end of every active axis, so stencil and kernel taps need no bounds tests.
+__host__ __device__ inline int coarse_padded(int dim, const int n[3]) {
+  return (n[0] + 2) * (dim == 3 ? n[1] + 2 : 1) * (n[2] + 2);
 }
 
-// sum_o K[o] u(c+o), or with SCALE sum_o K[o] isq(c+o) u(c+o)
-template <int DIM, bool SCALE>
-__device__ __forceinline__ float conv_s(const LV& M, const Kern& K, int i, int j, int k,
-                                        const float* u) {
+// A coarse level as the block sees it: couplings and scales unpadded (global
+// order), x and res padded with pitches px (y) and pz (z).
+template <int DIM>
+struct CoarseGeo {
+  int nx, ny, nz, px, pz;
+  const float *fx, *fy, *fz, *isq;
+  __device__ __forceinline__ int pad(int i, int j, int k) const {
+    return (i + 1) + (DIM == 3 ? px * (j + 1) : 0) + pz * (k + 1);
+  }
+};
+
+// (A x)(c) of a padded x at pc; cell c = i + nx * rest, rest = j + ny * k.
+// The arithmetic is coef() / apply7() of the grid kernels, with the x, y and
+// z couplings read at x faces c + rest, y faces c + nx k and z faces c.
+template <int DIM>
+__device__ __forceinline__ float coarse_lap(const CoarseGeo<DIM>& G, int c, int rest, int k, int pc,
+                                            const float* x) {
+  C7 co;
+  co.xl = G.fx[c + rest];
+  co.xh = G.fx[c + rest + 1];
+  if (DIM == 3) {
+    co.yl = G.fy[c + G.nx * k];
+    co.yh = G.fy[c + G.nx * k + G.nx];
+  } else {
+    co.yl = co.yh = 0.f;
+  }
+  co.zl = G.fz[c];
+  co.zh = G.fz[c + G.nx * G.ny];
+  co.d = ((co.xl + co.xh) + (co.yl + co.yh)) + (co.zl + co.zh);
+  const float s = DIM == 3 ? x[pc - G.px] : 0.f, n = DIM == 3 ? x[pc + G.px] : 0.f;
+  return apply7(co, x[pc], x[pc - 1], x[pc + 1], s, n, x[pc - G.pz], x[pc + G.pz]);
+}
+
+// sum_o K[o] u(pc + o) over a padded u, taps in (dz, dy, dx) order; a tap
+// in the halo adds K[o] * 0.
+template <int DIM>
+__device__ __forceinline__ float coarse_conv(const CoarseGeo<DIM>& G, const Kern& K, int pc,
+                                             const float* u) {
   float s = 0.f;
 #pragma unroll
   for (int dk = -1; dk <= 1; ++dk) {
-    const int kk = k + dk;
-    if (kk < 0 || kk >= M.nz) continue;
 #pragma unroll
     for (int dj = (DIM == 2 ? 0 : -1); dj <= (DIM == 2 ? 0 : 1); ++dj) {
-      const int jj = j + dj;
-      if (jj < 0 || jj >= M.ny) continue;
-      const int rowq = M.nx * (jj + M.ny * kk);
+      const float* row = u + pc + dk * G.pz + dj * G.px;
 #pragma unroll
-      for (int di = -1; di <= 1; ++di) {
-        const int ii = i + di;
-        if (ii < 0 || ii >= M.nx) continue;
-        const int q = ii + rowq;
-        const float v = SCALE ? M.isq[q] * u[q] : u[q];
-        s += K.w[(dk + 1) * 9 + (dj + 1) * 3 + (di + 1)] * v;
-      }
+      for (int di = -1; di <= 1; ++di) s += K.w[(dk + 1) * 9 + (dj + 1) * 3 + (di + 1)] * row[di];
     }
   }
   return s;
 }
 
-// The block-resident tail of the V-cycle: levels cf.. with their faces,
-// scales and vectors in shared memory.  Same layers as the grid kernels;
-// the smoothing residual is stored pre-scaled (u = D^-1/2 res), cell
-// coordinates come from a float reciprocal (exact below 2^22 cells), and the
-// coarsest level's damped-Jacobi sweeps run on only the warps that own its
-// cells (a named barrier instead of the whole block).
+// The block-resident tail of the V-cycle: levels cf.. with their couplings,
+// scales and vectors in shared memory (the couplings, scales and the first
+// level's residual brought in by cp.async, 16 bytes a copy).  Same layers as
+// the grid kernels; the first smoothing's scaled residual isq r is formed
+// once per cell instead of once per tap, x and res carry a zero halo, and
+// all indexing is 32-bit: the kernel runs on one SM and is bound by its
+// instruction issue.  Cell coordinates come from a float reciprocal (exact
+// below 2^22 cells); the coarsest level's damped-Jacobi sweeps run on only
+// the warps that own its cells (a named barrier instead of the whole block).
 template <int DIM>
 __global__ void __launch_bounds__(kCoarseThreads) k_coarse(CoarsePlan P) {
-  pdl_enter();
   extern __shared__ float4 smem4[];
   float* sm = reinterpret_cast<float*>(smem4);
   const int tid = threadIdx.x, nt = blockDim.x;
+  // zero the padded vectors (their halos stay zero)
   for (int l = 0; l < P.count; ++l) {
     const CoarseLevel& c = P.lv[l];
-    const int nf[3] = {(c.n[0] + 1) * c.n[1] * c.n[2], c.n[0] * (c.n[1] + 1) * c.n[2],
-                       c.n[0] * c.n[1] * (c.n[2] + 1)};
-    for (int a = 0; a < 3; ++a) {
-      if (DIM == 2 && a == 1) continue;
-      const float* src = c.f[a];
-      float* dst = sm + c.off[a];
-#pragma unroll 4
-      for (int q = tid; q < nf[a]; q += nt) dst[q] = src[q];
+    const int words = (coarse_padded(DIM, c.n) + 3) >> 2;
+    float4* x4 = reinterpret_cast<float4*>(sm + c.off[4]);
+    float4* r4 = reinterpret_cast<float4*>(sm + c.off[6]);
+    for (int q = tid; q < words; q += nt) {
+      x4[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+      r4[q] = make_float4(0.f, 0.f, 0.f, 0.f);
     }
-#pragma unroll 4
-    for (int q = tid; q < c.cells; q += nt) sm[c.off[3] + q] = c.isq[q];
   }
-  for (int q = tid; q < P.lv[0].cells; q += nt) sm[P.lv[0].off[5] + q] = P.lv[0].r_glob[q];
+  pdl_enter();
+  // 16-byte copies over the body of each array (every source is its own
+  // allocation, every destination 16-byte aligned), 4-byte ones for the tail
+  auto fetch = [&](float* dst, const float* src, int count) {
+    const int body = count & ~3;
+    for (int q = 4 * tid; q < body; q += 4 * nt) cp16(dst + q, src + q, true);
+    for (int q = body + tid; q < count; q += nt) cp4(dst + q, src + q, true);
+  };
+  for (int l = 0; l < P.count; ++l) {
+    const CoarseLevel& c = P.lv[l];
+    fetch(sm + c.off[0], c.f[0], (c.n[0] + 1) * c.n[1] * c.n[2]);
+    if (DIM == 3) fetch(sm + c.off[1], c.f[1], c.n[0] * (c.n[1] + 1) * c.n[2]);
+    fetch(sm + c.off[2], c.f[2], c.n[0] * c.n[1] * (c.n[2] + 1));
+    fetch(sm + c.off[3], c.isq, c.cells);
+  }
+  fetch(sm + P.lv[0].off[5], P.lv[0].r_glob, P.lv[0].cells);
+  cp_commit();
+  cp_wait<0>();
   __syncthreads();
   auto level = [&](int l) {
     const CoarseLevel& c = P.lv[l];
-    return LV{c.n[0], c.n[1], c.n[2], sm + c.off[0], DIM == 3 ? sm + c.off[1] : nullptr,
-              sm + c.off[2], sm + c.off[3]};
+    CoarseGeo<DIM> G;
+    G.nx = c.n[0];
+    G.ny = c.n[1];
+    G.nz = c.n[2];
+    G.px = c.n[0] + 2;
+    G.pz = DIM == 3 ? G.px * (c.n[1] + 2) : G.px;
+    G.fx = sm + c.off[0];
+    G.fy = DIM == 3 ? sm + c.off[1] : nullptr;
+    G.fz = sm + c.off[2];
+    G.isq = sm + c.off[3];
+    return G;
   };
-  auto cells_of = [&](const LV& M, auto f) {
-    const int cells = M.nx * M.ny * M.nz;
-    const float inx = 1.0f / (float)M.nx, iny = 1.0f / (float)M.ny;
+  // f(i, j, k, c, rest, pc) for every cell of G, strided over the block
+  auto cells_of = [&](const CoarseGeo<DIM>& G, auto f) {
+    const int cells = G.nx * G.ny * G.nz;
+    const float inx = 1.0f / (float)G.nx, iny = 1.0f / (float)G.ny;
     for (int c = tid; c < cells; c += nt) {
       const int rest = __float2int_rz(((float)c + 0.5f) * inx);
-      const int i = c - rest * M.nx;
-      const int k = __float2int_rz(((float)rest + 0.5f) * iny);
-      f(i, rest - k * M.ny, k, c);
+      const int i = c - rest * G.nx;
+      const int k = DIM == 3 ? __float2int_rz(((float)rest + 0.5f) * iny) : rest;
+      const int j = DIM == 3 ? rest - k * G.ny : 0;
+      f(i, j, k, c, rest, G.pad(i, j, k));
     }
   };
   const int last = P.count - 1;
   for (int l = 0; l < last; ++l) {
-    const LV M = level(l);
+    const CoarseGeo<DIM> G = level(l);
     float* x = sm + P.lv[l].off[4];
     const float* r = sm + P.lv[l].off[5];
     float* res = sm + P.lv[l].off[6];
     const Kern& K = P.K[l];
-    cells_of(M, [&](int i, int j, int k, int c) { x[c] = M.isq[c] * conv_s<DIM, true>(M, K, i, j, k, r); });
+    cells_of(G, [&](int, int, int, int c, int, int pc) { res[pc] = G.isq[c] * r[c]; });
+    __syncthreads();
+    cells_of(G, [&](int, int, int, int c, int, int pc) { x[pc] = G.isq[c] * coarse_conv<DIM>(G, K, pc, res); });
     __syncthreads();
     for (int s = 1; s < P.nu; ++s) {
-      cells_of(M, [&](int i, int j, int k, int c) { res[c] = M.isq[c] * (r[c] - lap_s<DIM>(M, i, j, k, c, x)); });
+      cells_of(G, [&](int, int, int k, int c, int rest, int pc) {
+        res[pc] = G.isq[c] * (r[c] - coarse_lap<DIM>(G, c, rest, k, pc, x));
+      });
       __syncthreads();
-      cells_of(M, [&](int i, int j, int k, int c) { x[c] += M.isq[c] * conv_s<DIM, false>(M, K, i, j, k, res); });
+      cells_of(G, [&](int, int, int, int c, int, int pc) { x[pc] += G.isq[c] * coarse_conv<DIM>(G, K, pc, res); });
       __syncthreads();
     }
-    cells_of(M, [&](int i, int j, int k, int c) { res[c] = r[c] - lap_s<DIM>(M, i, j, k, c, x); });
+    cells_of(G, [&](int, int, int k, int c, int rest, int pc) { res[pc] = r[c] - coarse_lap<DIM>(G, c, rest, k, pc, x); });
     __syncthreads();
-    const LV Cc = level(l + 1);
+    // restriction: the sum over the 2 x 2 (x 2) children, (z, y, x) order;
+    // children past an odd edge are halo zeros
+    const CoarseGeo<DIM> C = level(l + 1);
     float* rc = sm + P.lv[l + 1].off[5];
-    cells_of(Cc, [&](int ci, int cj, int ck, int qc) {
+    cells_of(C, [&](int ci, int cj, int ck, int qc, int, int) {
       float s = 0.f;
+#pragma unroll
       for (int u = 0; u < 2; ++u)
-        for (int v = 0; v < 2; ++v)
-          for (int t = 0; t < 2; ++t) {
-            const int i = 2 * ci + t, j = 2 * cj + v, k = 2 * ck + u;
-            if (i < M.nx && j < M.ny && k < M.nz) s += res[i + M.nx * (j + M.ny * k)];
-          }
+#pragma unroll
+        for (int v = 0; v < (DIM == 3 ? 2 : 1); ++v)
+#pragma unroll
+          for (int t = 0; t < 2; ++t) s += res[G.pad(2 * ci + t, 2 * cj + v, 2 * ck + u)];
       rc[qc] = s;
     });
     __syncthreads();
   }
   {
-    const LV M = level(last);
+    const CoarseGeo<DIM> G = level(last);
     float* x = sm + P.lv[last].off[4];
     const float* r = sm + P.lv[last].off[5];
     float* res = sm + P.lv[last].off[6];
-    const int cells = M.nx * M.ny * M.nz;
+    const int cells = G.nx * G.ny * G.nz;
     const int nw = min(32, (cells + 31) / 32);  // warps that own the coarsest cells
     if (tid < 32 * nw) {
       auto wsync = [&]() {
         if (nw == 1) __syncwarp();
         else asm volatile("bar.sync 1, %0;" ::"r"(32 * nw) : "memory");
       };
-      const float inx = 1.0f / (float)M.nx, iny = 1.0f / (float)M.ny;
-      for (int c = tid; c < cells; c += 32 * nw) x[c] = 0.f;
-      wsync();
+      const float inx = 1.0f / (float)G.nx, iny = 1.0f / (float)G.ny;
       for (int s = 0; s < P.sweeps; ++s) {
         for (int c = tid; c < cells; c += 32 * nw) {
           const int rest = __float2int_rz(((float)c + 0.5f) * inx);
-          const int i = c - rest * M.nx;
-          const int k = __float2int_rz(((float)rest + 0.5f) * iny);
-          res[c] = r[c] - lap_s<DIM>(M, i, rest - k * M.ny, k, c, x);
+          const int i = c - rest * G.nx;
+          const int k = DIM == 3 ? __float2int_rz(((float)rest + 0.5f) * iny) : rest;
+          const int pc = G.pad(i, DIM == 3 ? rest - k * G.ny : 0, k);
+          res[pc] = r[c] - coarse_lap<DIM>(G, c, rest, k, pc, x);
         }
         wsync();
         for (int c = tid; c < cells; c += 32 * nw) {
-          const float is = M.isq[c];
-          x[c] += 0.8f * (is * is) * res[c];
+          const int rest = __float2int_rz(((float)c + 0.5f) * inx);
+          const int i = c - rest * G.nx;
+          const int k = DIM == 3 ? __float2int_rz(((float)rest + 0.5f) * iny) : rest;
+          const int pc = G.pad(i, DIM == 3 ? rest - k * G.ny : 0, k);
+          const float is = G.isq[c];
+          x[pc] += 0.8f * (is * is) * res[pc];
         }
         wsync();
       }
@@ -747,24 +826,28 @@ __global__ void __launch_bounds__(kCoarseThreads) k_coarse(CoarsePlan P) {
     __syncthreads();
   }
   for (int l = last - 1; l >= 0; --l) {
-    const LV M = level(l);
-    const LV Cc = level(l + 1);
+    const CoarseGeo<DIM> G = level(l);
+    const CoarseGeo<DIM> C = level(l + 1);
     float* x = sm + P.lv[l].off[4];
     const float* r = sm + P.lv[l].off[5];
     float* res = sm + P.lv[l].off[6];
     const float* ec = sm + P.lv[l + 1].off[4];
     const float cw = P.cw[l];
     const Kern& K = P.K[l];
-    cells_of(M, [&](int i, int j, int k, int c) { x[c] += cw * ec[parent(Cc, i, j, k)]; });
+    cells_of(G, [&](int i, int j, int k, int, int, int pc) { x[pc] += cw * ec[C.pad(i >> 1, j >> 1, k >> 1)]; });
     __syncthreads();
     for (int s = 0; s < P.nu; ++s) {
-      cells_of(M, [&](int i, int j, int k, int c) { res[c] = M.isq[c] * (r[c] - lap_s<DIM>(M, i, j, k, c, x)); });
+      cells_of(G, [&](int, int, int k, int c, int rest, int pc) {
+        res[pc] = G.isq[c] * (r[c] - coarse_lap<DIM>(G, c, rest, k, pc, x));
+      });
       __syncthreads();
-      cells_of(M, [&](int i, int j, int k, int c) { x[c] += M.isq[c] * conv_s<DIM, false>(M, K, i, j, k, res); });
+      cells_of(G, [&](int, int, int, int c, int, int pc) { x[pc] += G.isq[c] * coarse_conv<DIM>(G, K, pc, res); });
       __syncthreads();
     }
   }
-  for (int q = tid; q < P.lv[0].cells; q += nt) P.lv[0].x_glob[q] = sm[P.lv[0].off[4] + q];
+  const CoarseGeo<DIM> G0 = level(0);
+  const float* x0 = sm + P.lv[0].off[4];
+  cells_of(G0, [&](int, int, int, int c, int, int pc) { P.lv[0].x_glob[c] = x0[pc]; });
 }
 
 // ------------------------------------------------------ hierarchy build
@@ -871,7 +954,7 @@ size_t coarse_bytes(const MgHierarchy& H, int from) {
     const MgLevel& M = H.L[l];
     floats += up4((int64_t)(M.n[0] + 1) * M.n[1] * M.n[2]) + up4((int64_t)M.n[0] * M.n[1] * (M.n[2] + 1));
     if (H.dim == 3) floats += up4((int64_t)M.n[0] * (M.n[1] + 1) * M.n[2]);
-    floats += 4 * up4(M.cells);
+    floats += 2 * up4(M.cells) + 2 * up4(coarse_padded(H.dim, M.n));
   }
   return floats * sizeof(float);
 }
@@ -900,7 +983,10 @@ CoarsePlan coarse_plan(const MgHierarchy& H, const MgWeights& W) {
     c.off[0] = take((int64_t)(c.n[0] + 1) * c.n[1] * c.n[2]);
     c.off[1] = H.dim == 3 ? take((int64_t)c.n[0] * (c.n[1] + 1) * c.n[2]) : 0;
     c.off[2] = take((int64_t)c.n[0] * c.n[1] * (c.n[2] + 1));
-    for (int s = 3; s < 7; ++s) c.off[s] = take(c.cells);
+    c.off[3] = take(c.cells);                          // isq
+    c.off[4] = take(coarse_padded(H.dim, c.n));        // x (padded)
+    c.off[5] = take(c.cells);                          // r
+    c.off[6] = take(coarse_padded(H.dim, c.n));        // res (padded)
     P.K[q] = kern_of(W, H.coarse_from + q);
     P.cw[q] = cw_of(W, H.coarse_from + q);
   }

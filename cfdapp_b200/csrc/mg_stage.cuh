@@ -11,29 +11,8 @@
 // measured slower there).
 #pragma once
 
-// 16-, 8- and 4-byte asynchronous global -> shared copies (cp.async); a copy
-// whose source lies outside the level fills its bytes with zeros and reads
-// nothing.  One commit group per staged plane.
-__device__ __forceinline__ void cp16(void* dst, const void* src, bool in) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(src), "r"(in ? 16 : 0)
-               : "memory");
-}
-__device__ __forceinline__ void cp8(void* dst, const void* src, bool in) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(src), "r"(in ? 8 : 0)
-               : "memory");
-}
-__device__ __forceinline__ void cp4(void* dst, const void* src, bool in) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(src), "r"(in ? 4 : 0)
-               : "memory");
-}
-__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
-}
+// The cp.async helpers (cp16 / cp8 / cp4, cp_commit, cp_wait) are defined
+// in mg.cu ahead of the coarse-level block, which uses them too.
 
 // Staged plane tile of a quad pass (3D: 32 x 8 threads, a 128 x 8 patch): a
 // slot holds rows gj = tiy*TY - 1 .. tiy*TY + TY of x in [x0 - 4, x0 + 132)
