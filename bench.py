@@ -82,6 +82,13 @@ def grids_from(a):
     return tuple(out)
 
 
+def pprime_workload(grids):
+    """The workload name of the isolated p' solve on `grids` (both arms)."""
+    names = " + ".join(f"{5 if d == 2 else 7}-point {n}^{d}" for d, n in grids)
+    return (f"isolated p' solve: {names}, Neumann + pinned cell, seeded 32-sinusoid RHS, x0=0, "
+            "rel-res 1e-8 (FP64-verified)")
+
+
 def dist_info():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -310,9 +317,7 @@ def run_reference(a, grids):
             "warmup": a.warmup, "ms_per_step": value, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": "isolated p' solve: 5-point 2048^2 + 7-point 256^3, "
-                                   "Neumann + pinned cell, seeded 32-sinusoid RHS, x0=0, "
-                                   "rel-res 1e-8 (FP64-verified)",
+            "config": {"workload": pprime_workload(grids),
                        "grids": [f"{d}D {n}" for d, n in grids]},
             "cpu_baseline": {"value": value, "unit": "ms", "cores": cores, "kind": "reference",
                              "sample": sample},
@@ -925,9 +930,7 @@ def main():
             "warmup": a.warmup, "ms_per_step": ms_step, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64 (FCG) / f32 (V-cycle)",
             "data": "synthetic",
-            "config": {"workload": "isolated p' solve: 5-point 2048^2 + 7-point 256^3, "
-                                   "Neumann + pinned cell, seeded 32-sinusoid RHS, x0=0, "
-                                   "rel-res 1e-8 (FP64-verified)",
+            "config": {"workload": pprime_workload(grids),
                        "solver": "FP64 flexible CG + learned FP32 V-cycle preconditioner "
                                  "(CUDA graph WHILE loop)",
                        "grids": [f"{d}D {n}" for d, n in grids],
