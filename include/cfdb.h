@@ -75,7 +75,10 @@ typedef struct {
 enum { CFDB_KRYLOV_CG = 0, CFDB_KRYLOV_BICGSTAB = 1 };
 enum {
   CFDB_PRECISION_FP64 = 0,          /* every sweep in FP64 (the reference's arithmetic) */
-  CFDB_PRECISION_FP32_REFINED = 1   /* FP32 inner sweeps inside FP64 iterative refinement */
+  CFDB_PRECISION_FP32_REFINED = 1   /* mixed precision: FP32 directions, FP64 iterate and
+                                       residual with residual replacement (one Krylov space;
+                                       rows a multiple of 16 bytes in FP32), else FP32 inner
+                                       solves inside FP64 iterative refinement */
 };
 enum {
   CFDB_PRECOND_NONE = 0,
@@ -92,8 +95,10 @@ typedef struct {
   double abs_tol;         /* ||r||_2 <= abs_tol, or */
   double rel_tol;         /* ||r||_2 / ||r0||_2 <= rel_tol (unpreconditioned residual) */
   int64_t max_iterations; /* FP64: Krylov iterations; FP32_REFINED: total inner iterations */
-  double inner_rel_tol;   /* FP32_REFINED: reduction asked of each inner solve (0 = default) */
-  int64_t max_refinements;/* FP32_REFINED: outer FP64 refinement steps (0 = default) */
+  double inner_rel_tol;   /* FP32_REFINED: residual drop between FP64 residual replacements
+                             (default 0.1), or the reduction asked of each inner solve of the
+                             refinement form (default 1e-4); 0 = default */
+  int64_t max_refinements;/* FP32_REFINED, refinement form: outer FP64 steps (0 = default) */
 } cfdb_linear_settings;
 
 /* SolverResult (LinearSolver.hpp:110-134) plus refinement counters. */
@@ -103,7 +108,8 @@ typedef struct {
   double initial_residual;    /* ||b - A x0||_2 */
   double final_residual;      /* ||b - A x||_2 as the method tracks it */
   double true_residual;       /* FP64-recomputed ||b - A x||_2 of the returned x */
-  int64_t refinements;        /* FP32_REFINED: outer FP64 steps taken */
+  int64_t refinements;        /* FP32_REFINED: FP64 residual replacements (refinement form:
+                                 outer FP64 steps) taken */
   int64_t restarts;           /* BiCGSTAB restarts */
   double device_ms;           /* device time of the solve (CUDA events, launching stream) */
   int64_t kernel_launches;    /* kernels this library launched for the solve */
