@@ -50,8 +50,6 @@ class Op2D:
         self.xl, self.xh = fx[:, :-1].clone(), fx[:, 1:].clone()
         self.yl, self.yh = fy[:-1, :].clone(), fy[1:, :].clone()
         self.diag = ((self.xl + self.xh) + self.yl) + self.yh
-        for t in (self.xl, self.xh, self.yl, self.yh):
-            pass
         self.xl[:, 0] = 0.0
         self.xh[:, -1] = 0.0
         self.yl[0, :] = 0.0
