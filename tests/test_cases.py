@@ -10,7 +10,7 @@ import shutil
 import numpy as np
 import pytest
 
-from cfdapp_b200 import cases, cfdb
+from cfdapp_b200 import cases
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
 CASES = os.path.join(GOLDEN, "cases")
